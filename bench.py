@@ -1,0 +1,324 @@
+"""Benchmark of the B200 TILD hot path: particle-steps/s on one system per GPU.
+
+Workload (default, --workload blend): A/B homopolymer blend, 130,000 chains x N=20 = 2.6M beads,
+box 64^3, grid 128^3, three gaussian_erf pair styles (R_p = 0.5, smearing 0.5, kappa = 50,
+chi = 0.2), 4th-order assignment (64-point stencil), GJF, dt = 0.005, seeded synthetic chains.
+A "step" is one full TILD step: spread, R2C, k-space multiply, C2R, gather + bonds + GJF.
+
+Arms:
+  --impl ours       (default) libtild through its C ABI.  value: device-timed (CUDA events on
+                    the context stream) K steps with the state resident in HBM; e2e: the same K
+                    steps through the public API from host buffers (initial state uploaded, an
+                    observable record read back every 100 steps, final positions read back).
+  --impl reference  the reference algorithm on the host cores: the FP64 oracle port
+                    (oracle/tild_oracle.c, OpenMP over all host threads) on a bounded sample of
+                    the same workload.  When the reference's own CUDA build is present
+                    (oracle/_ref/gpu-tild) its particle-steps/s on this GPU is added as
+                    "reference_cuda".
+Multi-GPU (torchrun, N > 1): one independent replica per GPU (systems do not exchange
+anything), timing = max over ranks, value = total particle-steps of all ranks / that time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "gpu-tild_b200")]
+
+import numpy as np  # noqa: E402
+
+import tild  # noqa: E402
+import tild_systems as ts  # noqa: E402
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+C_SIZEOF_OBS = __import__("ctypes").sizeof(tild.Obs)
+
+
+def make_system(workload: str):
+    if workload == "blend":
+        return ts.homopolymer_blend(), "blend_2.6M_128^3_gaussian_erf_p3_GJF"
+    if workload == "diblock":
+        return ts.diblock_melt(), "diblock_40k_40^3_gaussian_p1_GJF"
+    if workload == "coacervate":
+        return ts.coacervate(), "coacervate_220k_96^3_charges_gaussian_p1_EM"
+    raise SystemExit(f"unknown workload {workload}")
+
+
+# ------------------------------------------------------------------------------------------
+# algorithmic bytes per launch of each stage (the roofline numerators)
+# ------------------------------------------------------------------------------------------
+def stage_bytes(s) -> dict:
+    ns, D, T = s.ns, s.dim, s.ntypes
+    C = 1 if s.charges is not None else 0
+    M = int(np.prod(s.nx[:D]))
+    Mh = M // s.nx[0] * (s.nx[0] // 2 + 1)
+    nfft = sum(1 for st in s.styles if st.kind != tild.STYLE_FIELDPHASE)
+    gjf = any(k == tild.INTEGRATOR_GJF for k, _ in s.integrators)
+    per_bead_gather = 16 + 4 + 12 + 16 + 16 + (24 if gjf else 0) + (4 if C else 0)
+    return {
+        "zero": (T + C) * M * 4,
+        "spread": ns * (16 + (4 if C else 0)) + (T + C) * M * 4,
+        "r2c": (T + C) * (M * 4 + Mh * 8),
+        "kmul": (T + C) * Mh * 8 + nfft * Mh * 4 + (C * Mh * 4) + (T + C) * D * Mh * 8,
+        "c2r": (T + C) * D * (Mh * 8 + M * 4),
+        "fieldphase": 0,
+        "gather": ns * per_bead_gather + (T + C) * D * M * 4,
+    }
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for k, v in zip(names, r[3:7]):
+                    if v.strip() == "Active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 0, 1
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return dist, rank, local, ws
+
+
+def dist_max(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------
+def run_ours(args):
+    dist, rank, local, ws = dist_setup(args.gpus)
+    s, wname = make_system(args.workload)
+    ctx = tild.Context(s, device=local)
+    launches0 = ctx.kernel_launches()
+    ctx.step(args.warmup)
+    ctx.sync()
+    dist_barrier(dist)
+    with ClockSampler(local) as clk:
+        l0 = ctx.kernel_launches()
+        ms = ctx.time_steps(args.steps)
+        launches = ctx.kernel_launches() - l0
+    ms = dist_max(dist, ms)
+    clocks = clk.summary()
+    per_rank = s.ns * args.steps
+    value = per_rank * ws / (ms / 1e3)
+
+    # per-stage times over the same number of steps -> roofline of the dominant kernel
+    prof = ctx.profile_steps(args.steps)
+    sb = stage_bytes(s)
+    dom = max(prof, key=lambda k: prof[k])
+    dom_ms = prof[dom] / args.steps
+    peak, peak_kind = hbm_peak()
+    achieved = sb[dom] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+
+    # end to end through the public API from host buffers
+    e2e_steps = args.steps
+    log_freq = 100
+    t0 = time.perf_counter()
+    ctx.set_state(s.x)
+    done = 0
+    obs_reads = 0
+    while done < e2e_steps:
+        n = min(log_freq, e2e_steps - done)
+        ctx.step(n)
+        done += n
+        if done % log_freq == 0:
+            ctx.observables()
+            obs_reads += 1
+    xf, _, _ = ctx.get_state()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(dist, e2e_s)
+    obs_bytes = C_SIZEOF_OBS
+    h2d = s.ns * s.dim * 4
+    d2h = s.ns * s.dim * 4 + obs_reads * obs_bytes
+    e2e = {"value": per_rank * ws / e2e_s, "unit": "particle-steps/s",
+           "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+           "note": "public C ABI from host arrays: upload state, K steps, observables every 100 steps, "
+                   "download positions"}
+
+    out = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random-walk chains)",
+        "config": {"workload": wname, "ns_per_gpu": s.ns, "grid": list(s.nx[:s.dim]), "pmeorder": s.pmeorder,
+                   "pair_styles": len(s.styles), "integrator": "GJF" if s.integrators[0][0] else "EM",
+                   "parallelism": f"replicas{ws}",
+                   "l2": "per-step working set (positions, grids, spectra) exceeds the 126 MB L2"},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "stages_ms_per_step": {k: v / args.steps for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} ({'MEASURED_PEAKS.json' if peak_kind == 'measured' else 'fallback'})",
+                     "algorithmic_bytes_per_launch": sb[dom], "traffic": None},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(s, args)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def cpu_baseline(s, args, target_s: float = 20.0):
+    """FP64 oracle on the host cores: whole steps of the same system, as many as fit ~target_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    o = oracle.Oracle(s)
+    cores = oracle.max_threads()
+    x, xo, nz = s.x.copy(), s.x.copy(), np.zeros_like(s.x)
+    t0 = time.perf_counter()
+    o.step(x, xo, nz, 1, True)
+    t1 = time.perf_counter() - t0
+    k = max(1, min(int(target_s / max(t1, 1e-3)), 50))
+    t0 = time.perf_counter()
+    for i in range(k):
+        o.step(x, xo, nz, 2 + i, True)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": s.ns * k / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{k} full steps of the same {s.ns}-bead system after 1 untimed step "
+                      f"(oracle/tild_oracle.c, FP64, OpenMP {cores} threads)"}
+
+
+def reference_cuda(s, wname, steps=(20, 120)):
+    """The reference program built from its own sources (oracle/_ref/gpu-tild) on this GPU:
+    per-step time = difference of wall times of two runs that differ only in max_steps."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "gpu-tild")
+    if not os.path.exists(exe):
+        return None
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        ts.write_data_file(os.path.join(td, "input.data"), s)
+        for n in steps:
+            ts.write_input_script(os.path.join(td, "input"), s, max_steps=n, log_freq=10 ** 8, binary_freq=0)
+            t0 = time.perf_counter()
+            r = subprocess.run([exe, "-in", "input"], cwd=td, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                               timeout=900)
+            times.append(time.perf_counter() - t0)
+            if r.returncode != 0:
+                return {"unavailable": f"reference build exited {r.returncode}"}
+    per_step = (times[1] - times[0]) / (steps[1] - steps[0])
+    return {"value": s.ns / per_step, "unit": "particle-steps/s", "ms_per_step": per_step * 1e3,
+            "binary": "oracle/_ref/gpu-tild (unmodified reference sources, nvcc -arch=sm_100a -O3)",
+            "method": f"wall-time difference of {steps[1]}- and {steps[0]}-step runs (setup and output cancel)"}
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if ws > 1 and rank != 0:
+        return
+    s, wname = make_system(args.workload)
+    cb = cpu_baseline(s, args, target_s=min(60.0, 4.0 * max(args.steps, 1)))
+    out = {"impl": "reference", "metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-walk chains)",
+           "config": {"workload": wname, "ns_per_gpu": s.ns, "grid": list(s.nx[:s.dim])},
+           "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    if not args.no_reference_cuda:
+        rc = reference_cuda(s, wname)
+        if rc is not None:
+            out["reference_cuda"] = rc
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
