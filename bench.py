@@ -65,7 +65,8 @@ def stage_bytes(s) -> dict:
     gjf = any(k == tild.INTEGRATOR_GJF for k, _ in s.integrators)
     per_bead_gather = 16 + 4 + 12 + 16 + 16 + (24 if gjf else 0) + (4 if C else 0)
     return {
-        "zero": (T + C) * M * 4,
+        "sort": 0,
+        "fix2float": (T + C) * M * (8 + 8 + 4),
         "spread": ns * (16 + (4 if C else 0)) + (T + C) * M * 4,
         "r2c": (T + C) * (M * 4 + Mh * 8),
         "kmul": (T + C) * Mh * 8 + nfft * Mh * 4 + (C * Mh * 4) + (T + C) * D * Mh * 8,

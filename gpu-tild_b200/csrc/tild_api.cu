@@ -77,7 +77,7 @@ int dalloc(tild_ctx* c, T** p, size_t n, const char* what) {
 void free_all(tild_ctx* c) {
   void* ptrs[] = {c->pos[0], c->pos[1], c->noise, c->bead_id, c->slot_of, c->bond_nbr, c->bond_info, c->charge,
                   c->bondk_dev, c->bondr_dev, c->types_dev, c->xorwow, c->rho, c->rhok, c->gk, c->gfield, c->utab,
-                  c->ctab, c->virk, c->frfield, c->kd, c->kk, c->red, c->xfer, c->d_status};
+                  c->ctab, c->virk, c->frfield, c->rho_fx, c->g4, c->kd, c->kk, c->red, c->xfer, c->d_status};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < TILD_MAX_COMPUTES; i++)
@@ -86,6 +86,7 @@ void free_all(tild_ctx* c) {
     cufftDestroy(c->plan_r2c);
     cufftDestroy(c->plan_c2r);
   }
+  tild_sort_free(c);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -271,6 +272,7 @@ int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
   }
 
   const size_t ns = c->ns, M = g.M, Mh = g.Mh;
+  c->spread_cap = 12288;
   const size_t nch = c->T + c->C;
   const size_t nfft = c->styles_k.size();
   int rc = TILD_OK;
@@ -286,9 +288,11 @@ int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
   rc = rc ? rc : dalloc(c, &c->bondr_dev, TILD_MAX_BOND_TYPES, "bond constants");
   if (c->C) rc = rc ? rc : dalloc(c, &c->charge, ns, "charges");
   rc = rc ? rc : dalloc(c, &c->rho, nch * M, "densities");
+  rc = rc ? rc : dalloc(c, &c->rho_fx, nch * M, "density accumulator");
   rc = rc ? rc : dalloc(c, &c->rhok, nch * Mh, "density spectra");
   rc = rc ? rc : dalloc(c, &c->gk, nch * c->D * Mh, "force spectra");
   rc = rc ? rc : dalloc(c, &c->gfield, nch * c->D * M, "force fields");
+  rc = rc ? rc : dalloc(c, &c->g4, nch * M, "interleaved force fields");
   rc = rc ? rc : dalloc(c, &c->utab, nfft * Mh, "multiplier tables");
   rc = rc ? rc : dalloc(c, &c->virk, nfft * c->nP * Mh, "virial tables");
   if (c->C) rc = rc ? rc : dalloc(c, &c->ctab, Mh, "charge table");
@@ -305,6 +309,7 @@ int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
     return rc;
   }
   cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->rho_fx, 0, sizeof(unsigned long long) * nch * M, c->stream);
   cudaMemsetAsync(c->noise, 0, sizeof(float) * ns * 3, c->stream);
   {
     std::vector<float> bk(TILD_MAX_BOND_TYPES, 0.f), br(TILD_MAX_BOND_TYPES, 0.f);
@@ -334,6 +339,8 @@ int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
     else
       c->plans = true;
   }
+  c->sort_interval = cfg->sort_interval == 0 ? 16 : (cfg->sort_interval < 0 ? 0 : cfg->sort_interval);
+  if (!rc && c->sort_interval > 0) rc = tild_sort_alloc(c);
   if (!rc) rc = tild_build_tables(c);
   if (rc) {
     fprintf(stderr, "tild_create: %s\n", c->err.c_str());
@@ -390,6 +397,33 @@ int32_t tild_set_topology(tild_ctx* c, const int32_t* types, const float* charge
       (c->C && tild_check(c, cudaMemcpyAsync(c->charge, q.data(), (size_t)ns * 4, cudaMemcpyHostToDevice, c->stream), "charges")) ||
       tild_check(c, cudaStreamSynchronize(c->stream), "sync topology"))
     return TILD_ERR_CUDA;
+  // fixed-point scale of the shared-memory spread: 256 beads x the largest product of stencil
+  // weights (times the largest |q| on the charge channel) must stay below 2^31
+  {
+    double wmax = 0.0;
+    for (int k = 0; k <= 1000; k++) {
+      const double sx = -0.5 + k / 1000.0;
+      double W[5];
+      const int P = c->p;
+      double sx2 = sx * sx, sx3, sx4;
+      if (P == 0) { W[0] = 1; }
+      else if (P == 1) { W[0] = 0.5 - sx; W[1] = 0.5 + sx; }
+      else if (P == 2) { W[0] = 0.125 - 0.5 * sx + 0.5 * sx2; W[1] = 0.75 - sx2; W[2] = 0.125 + 0.5 * sx + 0.5 * sx2; }
+      else if (P == 3) { sx3 = sx2 * sx; W[0] = (1 - 6 * sx + 12 * sx2 - 8 * sx3) / 48; W[1] = (23 - 30 * sx - 12 * sx2 + 24 * sx3) / 48;
+                         W[2] = (23 + 30 * sx - 12 * sx2 - 24 * sx3) / 48; W[3] = (1 + 6 * sx + 12 * sx2 + 8 * sx3) / 48; }
+      else { sx3 = sx2 * sx2; sx4 = sx2 * sx2; W[0] = (1 - 8 * sx + 24 * sx2 - 32 * sx3 + 16 * sx4) / 384;
+             W[1] = (19 - 44 * sx + 24 * sx2 + 16 * sx3 - 16 * sx4) / 96; W[2] = (115 - 120 * sx2 + 48 * sx4) / 192;
+             W[3] = (19 + 44 * sx + 24 * sx2 - 16 * sx3 - 16 * sx4) / 96; W[4] = (1 + 8 * sx + 24 * sx2 + 32 * sx3 + 16 * sx4) / 384; }
+      for (int a = 0; a <= P; a++) wmax = std::max(wmax, std::fabs(W[a]));
+    }
+    double qmax = 1.0;
+    if (c->C)
+      for (int b = 0; b < ns; b++) qmax = std::max(qmax, (double)std::fabs(charges[b]));
+    const double bound = 256.0 * std::pow(wmax * 1.05, c->D) / (double)c->g.gvol * qmax;
+    int k = 0;
+    while (k < 31 && bound * std::ldexp(1.0, k + 1) < 2147483647.0) k++;
+    c->spread_kbits = k;
+  }
   c->topo_set = true;
   return TILD_OK;
 }
@@ -417,6 +451,10 @@ int32_t tild_set_state(tild_ctx* c, const float* x, const float* xo, const float
   if (c->cfg.rng == TILD_RNG_XORWOW) {
     k_init_xorwow<<<nb, 256, 0, c->stream>>>(c->xorwow, c->bead_id, c->ns, (unsigned int)c->cfg.seed);
     c->launches++;
+  }
+  if (c->sort_interval > 0) {
+    int rs = tild_sort_beads(c);
+    if (rs) return rs;
   }
   if (tild_check(c, cudaStreamSynchronize(c->stream), "set state")) return TILD_ERR_CUDA;
   c->state_set = true;

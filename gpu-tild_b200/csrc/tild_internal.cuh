@@ -11,6 +11,7 @@
 //   rhok       cufftComplex[(T+C)*Mh] R2C of rho
 //   gk         cufftComplex[(T+C)*D*Mh] -i k_d Phi_t(k): input of the batched C2R
 //   gfield     float[(T+C)*D*M]      -grad of the convolved potential per type (and E field)
+//   g4         float4[(T+C)*M]       the same, interleaved per grid point for the gather
 //   utab       float[nfft_styles*Mh]  u_s(k)/M per FFT pair style
 //   virk       cufftComplex[nfft_styles*nP*Mh] virial kernels / M^2
 #pragma once
@@ -84,10 +85,12 @@ struct tild_ctx {
   curandStateXORWOW_t* xorwow = nullptr;
 
   // grids
+  unsigned long long* rho_fx = nullptr;  // fixed-point (2^32) density accumulator [(T+C)*M]
   float* rho = nullptr;
   cufftComplex* rhok = nullptr;
   cufftComplex* gk = nullptr;
   float* gfield = nullptr;
+  float4* g4 = nullptr;                  // interleaved force field [(T+C)][M] (gather input)
   float* utab = nullptr;
   float* ctab = nullptr;              // charge force multiplier [Mh]
   cufftComplex* virk = nullptr;
@@ -106,6 +109,29 @@ struct tild_ctx {
   cufftHandle plan_r2c = 0, plan_c2r = 0;
   bool plans = false;
 
+  // spatial sort of the slots (tild_sort.cu)
+  unsigned* sort_keys = nullptr;
+  unsigned* sort_keys_alt = nullptr;
+  int* sort_vals = nullptr;
+  int* sort_perm = nullptr;
+  int* sort_newslot = nullptr;
+  float4* alt_pos[2] = {nullptr, nullptr};
+  float* alt_noise = nullptr;
+  int* alt_bead_id = nullptr;
+  int* alt_info = nullptr;
+  int* alt_nbr = nullptr;
+  float* alt_charge = nullptr;
+  curandStateXORWOW_t* alt_xorwow = nullptr;
+  void* sort_temp = nullptr;
+  size_t sort_temp_bytes = 0;
+  int sort_bits = 0;
+  int sort_kg[7] = {0};
+  int sort_interval = 0;               // 0: never
+  int64_t last_sort_step = -1;
+  long long sorts = 0;
+  int spread_cap = 0;                  // shared-memory 32-bit words of the tiled spread
+  int spread_kbits = 20;               // fractional bits of the shared 32-bit fixed point
+
   // per-stage timing (tild_profile_steps): an event is recorded at every stage boundary
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_stage;
@@ -118,8 +144,8 @@ struct tild_ctx {
   std::string err;
 };
 
-enum TildStage { STAGE_ZERO = 0, STAGE_SPREAD, STAGE_R2C, STAGE_KMUL, STAGE_C2R, STAGE_FIELD, STAGE_GATHER, STAGE_COUNT };
-static const char* const kStageNames[STAGE_COUNT] = {"zero", "spread", "r2c", "kmul", "c2r", "fieldphase", "gather"};
+enum TildStage { STAGE_SORT = 0, STAGE_ZERO, STAGE_SPREAD, STAGE_R2C, STAGE_KMUL, STAGE_C2R, STAGE_FIELD, STAGE_GATHER, STAGE_COUNT };
+static const char* const kStageNames[STAGE_COUNT] = {"sort", "fix2float", "spread", "r2c", "kmul", "c2r", "fieldphase", "gather"};
 
 // Records the start of a stage when profiling (the next mark, or the final one, ends it).
 inline void tild_mark(tild_ctx* c, int stage) {
@@ -241,4 +267,7 @@ int tild_check(tild_ctx* c, cudaError_t e, const char* what);
 int tild_check_fft(tild_ctx* c, cufftResult r, const char* what);
 int tild_poll_status(tild_ctx* c);
 int tild_ensure_red(tild_ctx* c, int nvals, int nblocks);
+int tild_sort_alloc(tild_ctx* c);                     // tild_sort.cu
+void tild_sort_free(tild_ctx* c);
+int tild_sort_beads(tild_ctx* c);
 double tild_ramp_ratio(const tild_ctx* c, int fft_slot, int64_t step);

@@ -14,6 +14,7 @@
 //    discards exactly those modes;
 //  * stencil weights are recomputed in the gather rather than cached (no ns*S W/inds arrays).
 #include "tild_internal.cuh"
+#include <climits>
 
 namespace {
 
@@ -22,54 +23,215 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 // ---------------------------------------------------------------------------------------------
 // Spreading: d_charge_grid / d_charge_grid_charges (device_grid_utils.cu:111-343)
 // ---------------------------------------------------------------------------------------------
+// Tiled spreading for slot-sorted beads.  One CTA takes 256 consecutive slots; their stencil
+// nodes are accumulated into a shared-memory box (relative to the first bead, periodic offsets
+// folded into [-N/2, N/2]) and the box is added to the global grid once.  Accumulation is in
+// 64-bit fixed point (weight * 2^32, native integer atomics): integer sums do not depend on the
+// order of the additions, so the densities are bitwise reproducible whatever the slot order or
+// the scheduling, and carry ~1e-10 absolute error before the single FP32 rounding.  When the box
+// does not fit (unsorted or widely spread chunks) the CTA adds each node to the global
+// fixed-point grid directly.
+__device__ __forceinline__ int fold_rel(int r, int N) {
+  r %= N;
+  if (r < 0) r += N;
+  if (r > N / 2) r -= N;
+  return r;
+}
+
+__device__ __forceinline__ int pmod(int n, int N) {
+  n %= N;
+  return n < 0 ? n + N : n;
+}
+
+constexpr double kFix = 4294967296.0;           // 2^32
+constexpr int kMaxRows = 1024;                  // (y, z) rows of a shared-memory spread box
+constexpr double kInvFix = 1.0 / 4294967296.0;
+
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+  return (unsigned long long)__double2ll_rn((double)v * kFix);
+}
+
+// Chunk bounding box of the beads' stencil bases, relative to the chunk's first bead.
+// Returns false when no bead of the chunk is finite.  Every thread of the block must call it.
 template <int D, int P>
-__global__ void __launch_bounds__(256) k_spread(const float4* __restrict__ pos, const float* __restrict__ charge, int ns,
-                                               Geom g, float* __restrict__ rho, int T, int C, int* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ns) return;
-  const float4 p = pos[i];
-  const float xs[3] = {p.x, p.y, p.z};
-  if (!isfinite(p.x) || !isfinite(p.y) || (D == 3 && !isfinite(p.z))) {
-    atomicOr(status, ST_NONFINITE_POS);
-    return;
-  }
-  const int t = tild_type_of(p.w);
-  float W[3][P + 1];
-  int idx[3][P + 1];
+__device__ __forceinline__ bool chunk_box(bool ok, const int (&rel)[3], int* s_min, int* s_max, int (&mn)[3],
+                                          int (&ext)[3], long long& vol) {
+  const unsigned full = 0xffffffffu;
 #pragma unroll
   for (int d = 0; d < D; d++) {
-    const int b = axis_base<P>(xs[d], g.dx[d], W[d]);
-#pragma unroll
-    for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
+    const int a = __reduce_min_sync(full, ok ? rel[d] : INT_MAX);
+    const int b = __reduce_max_sync(full, ok ? rel[d] : INT_MIN);
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&s_min[d], a);
+      atomicMax(&s_max[d], b);
+    }
   }
-  float* rt = rho + (long long)t * g.M;
-  const float q = C ? charge[i] : 0.f;
-  float* rc = rho + (long long)T * g.M;
-  if (D == 3) {
+  __syncthreads();
+  if (s_max[0] < s_min[0]) return false;
+  vol = 1;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    mn[d] = d < D ? s_min[d] : 0;
+    ext[d] = d < D ? s_max[d] - s_min[d] + P + 1 : 1;
+    vol *= ext[d];
+  }
+  return true;
+}
+
+template <int D, int P>
+__device__ __forceinline__ void chunk_origin(const float4* __restrict__ pos, int i0, const Geom& g, int* s_g0,
+                                             int* s_min, int* s_max) {
+  if (threadIdx.x == 0) {
+    const float4 p0 = pos[i0];
+    const float x0[3] = {p0.x, p0.y, p0.z};
+    float Wd[P + 1];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      s_g0[d] = (d < D && isfinite(x0[d])) ? axis_base<P>(x0[d], g.dx[d], Wd) : 0;
+      s_min[d] = INT_MAX;
+      s_max[d] = INT_MIN;
+    }
+  }
+  __syncthreads();
+}
+
+template <int D, int P>
+__global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__ pos, const float* __restrict__ charge,
+                                                     int ns, Geom g, unsigned long long* __restrict__ rho_fx, int T,
+                                                     int C, int cap, int kbits, int* status) {
+  // shared box: 32-bit fixed point with 2^kbits per unit (native integer shared atomics); kbits is
+  // chosen per context so that 256 beads at the largest weight cannot overflow
+  extern __shared__ int smi[];
+  __shared__ int s_g0[3], s_min[3], s_max[3];
+  __shared__ long long s_row[kMaxRows];
+  const int i0 = blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
+  chunk_origin<D, P>(pos, i0, g, s_g0, s_min, s_max);
+  float W[3][P + 1];
+  int rel[3] = {0, 0, 0};
+  int t = 0;
+  float q = 0.f;
+  bool ok = false;
+  if (i < ns) {
+    const float4 p = pos[i];
+    const float xs[3] = {p.x, p.y, p.z};
+    ok = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
+    if (!ok) {
+      atomicOr(status, ST_NONFINITE_POS);
+    } else {
+      t = tild_type_of(p.w);
+      q = C ? charge[i] : 0.f;
+#pragma unroll
+      for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
+    }
+  }
+  int mn[3], ext[3];
+  long long vol;
+  if (!chunk_box<D, P>(ok, rel, s_min, s_max, mn, ext, vol)) return;
+  const int nch = T + C;
+  const long long M = g.M;
+  const float ig = 1.0f / g.gvol;
+  const bool qc = C && q != 0.f;
+  if (vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
+    const int tot = (int)vol * nch;
+    for (int k = threadIdx.x; k < tot; k += blockDim.x) smi[k] = 0;
+    __syncthreads();
+    if (ok) {
+      const float sc32 = ig * __int_as_float((127 + kbits) << 23);  // 2^kbits / gvol
+      int* st = smi + (long long)t * vol;
+      int* sq = smi + (long long)T * vol;
+#pragma unroll
+      for (int ix = 0; ix <= P; ix++)
+#pragma unroll
+        for (int iy = 0; iy <= P; iy++) {
+          const int rowl = (rel[1] - mn[1] + iy) * ext[0] + (rel[0] - mn[0] + ix);
+          const float wxy = W[0][ix] * W[1][iy] * sc32;
+          if (D == 3) {
+#pragma unroll
+            for (int iz = 0; iz <= P; iz++) {
+              const int l = (rel[2] - mn[2] + iz) * ext[1] * ext[0] + rowl;
+              const float W3 = wxy * W[2][iz];
+              atomicAdd(st + l, __float2int_rn(W3));
+              if (qc) atomicAdd(sq + l, __float2int_rn(W3 * q));
+            }
+          } else {
+            atomicAdd(st + rowl, __float2int_rn(wxy));
+            if (qc) atomicAdd(sq + rowl, __float2int_rn(wxy * q));
+          }
+        }
+    }
+    __syncthreads();
+    // flush: one warp per box row (y, z) and channel, lanes along x; exact shift to the 2^32 grid
+    const int rows_per = ext[1] * ext[2];
+    for (int yz = threadIdx.x; yz < rows_per; yz += blockDim.x) {
+      const int ly = yz % ext[1], lz = yz / ext[1];
+      s_row[yz] = (long long)g.nx[0] * (pmod(s_g0[1] + mn[1] + ly, g.nx[1]) +
+                                        (long long)g.nx[1] * (D == 3 ? pmod(s_g0[2] + mn[2] + lz, g.nx[2]) : 0));
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int bx = pmod(s_g0[0] + mn[0], g.nx[0]);
+    int xoff[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      int xg = bx + lane + 32 * k;
+      while (xg >= g.nx[0]) xg -= g.nx[0];
+      xoff[k] = xg;
+    }
+    const int sh = 32 - kbits;
+    for (int ch = 0; ch < nch; ch++) {
+      const int* sch = smi + (long long)ch * vol;
+      unsigned long long* gch = rho_fx + ch * M;
+      for (int yz = warp; yz < rows_per; yz += nwarps) {
+        const int* srow = sch + (long long)yz * ext[0];
+        unsigned long long* grow = gch + s_row[yz];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int lx = lane + 32 * k;
+          if (lx < ext[0]) {
+            const int v = srow[lx];
+            if (v != 0) atomicAdd(grow + xoff[k], (unsigned long long)((long long)v << sh));
+          }
+        }
+      }
+    }
+  } else if (ok) {
+    int idx[3][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+#pragma unroll
+      for (int a = 0; a <= P; a++) idx[d][a] = pmod(s_g0[d] + rel[d] + a, g.nx[d]);
+    unsigned long long* rt = rho_fx + (long long)t * M;
+    unsigned long long* rc = rho_fx + (long long)T * M;
 #pragma unroll
     for (int ix = 0; ix <= P; ix++)
 #pragma unroll
       for (int iy = 0; iy <= P; iy++) {
         const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
+        const float wxy = W[0][ix] * W[1][iy] * ig;
+        if (D == 3) {
 #pragma unroll
-        for (int iz = 0; iz <= P; iz++) {
-          const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
-          const float W3 = W[0][ix] * W[1][iy] * W[2][iz] / g.gvol;
-          atomicAdd(rt + m, W3);
-          if (C && q != 0.f) atomicAdd(rc + m, W3 * q);
+          for (int iz = 0; iz <= P; iz++) {
+            const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
+            const float W3 = wxy * W[2][iz];
+            atomicAdd(rt + m, to_fix(W3));
+            if (qc) atomicAdd(rc + m, to_fix(W3 * q));
+          }
+        } else {
+          atomicAdd(rt + row, to_fix(wxy));
+          if (qc) atomicAdd(rc + row, to_fix(wxy * q));
         }
       }
-  } else {
-#pragma unroll
-    for (int ix = 0; ix <= P; ix++)
-#pragma unroll
-      for (int iy = 0; iy <= P; iy++) {
-        const long long m = (long long)idx[1][iy] * g.nx[0] + idx[0][ix];
-        const float W3 = W[0][ix] * W[1][iy] / g.gvol;
-        atomicAdd(rt + m, W3);
-        if (C && q != 0.f) atomicAdd(rc + m, W3 * q);
-      }
   }
+}
+
+// fixed-point grid -> FP32 density, clearing the accumulator for the next step
+__global__ void k_fix_to_float(unsigned long long* __restrict__ fx, float* __restrict__ rho, long long n) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const long long v = (long long)fx[k];
+  rho[k] = (float)((double)v * kInvFix);
+  fx[k] = 0ull;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -199,21 +361,62 @@ struct GArgs {
   float bond_req[TILD_MAX_BOND_TYPES];
 };
 
+// Interleave the C2R output [(T+C)][D][M] into one float4 (-dPhi/dx, -dPhi/dy, -dPhi/dz, 0) per
+// grid point and channel, so the gather reads a stencil node with a single 16-byte load.
+__global__ void k_interleave(const float* __restrict__ planar, float4* __restrict__ g4, int nch, int D, long long M) {
+  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  for (int ch = 0; ch < nch; ch++) {
+    const float* src = planar + (long long)ch * D * M + m;
+    g4[(long long)ch * M + m] = make_float4(src[0], src[M], D == 3 ? src[2 * M] : 0.f, 0.f);
+  }
+}
+
+template <int D, int P>
+__device__ __forceinline__ void gather4(const float4* __restrict__ F, const float (&W)[3][P + 1],
+                                        const int (&idx)[3][P + 1], const Geom& g, float (&acc)[3]) {
+#pragma unroll
+  for (int ix = 0; ix <= P; ix++)
+#pragma unroll
+    for (int iy = 0; iy <= P; iy++) {
+      const float wxy = W[0][ix] * W[1][iy];
+      const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
+      if (D == 3) {
+#pragma unroll
+        for (int iz = 0; iz <= P; iz++) {
+          const float4 v = __ldg(F + row + (long long)idx[2][iz] * g.nx[1] * g.nx[0]);
+          const float w = wxy * W[2][iz];
+          acc[0] += v.x * w;
+          acc[1] += v.y * w;
+          acc[2] += v.z * w;
+        }
+      } else {
+        const float4 v = __ldg(F + row);
+        acc[0] += v.x * wxy;
+        acc[1] += v.y * wxy;
+      }
+    }
+}
+
 template <int D, int P, bool INTEG, bool XW>
-__global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ pos_in, float4* __restrict__ pos_io,
-                                               float* __restrict__ noise, const int* __restrict__ bead_id,
-                                               const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
-                                               const float* __restrict__ charge, const float* __restrict__ gfield,
-                                               Geom g, int T, int C, GArgs ga, float* __restrict__ f_out,
-                                               curandStateXORWOW_t* __restrict__ xw, int ns, int* status) {
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(const float4* __restrict__ pos_in, float4* __restrict__ pos_io,
+                                                  float* __restrict__ noise, const int* __restrict__ bead_id,
+                                                  const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
+                                                  const float* __restrict__ charge, const float4* __restrict__ g4,
+                                                  Geom g, int T, int C, GArgs ga, float* __restrict__ f_out,
+                                                  curandStateXORWOW_t* __restrict__ xw, int ns, int* status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ns) return;
   const float4 p = pos_in[i];
   float x[3] = {p.x, p.y, p.z};
-  const bool finite = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
-  float f[3] = {0.f, 0.f, 0.f};
+  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+    atomicOr(status, ST_NONFINITE_POS);
+    return;  // left in place; the host reports TILD_ERR_NAN
+  }
   const int t = tild_type_of(p.w);
-  if (finite) {
+  const long long M = g.M;
+  float f[3] = {0.f, 0.f, 0.f};
+  {
     float W[3][P + 1];
     int idx[3][P + 1];
 #pragma unroll
@@ -222,81 +425,40 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ pos_i
 #pragma unroll
       for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
     }
-    const long long M = g.M;
-    const float* G0 = gfield + (long long)t * D * M;
     if (C) {
       const float q = charge[i];
       if (q != 0.f) {
-        const float* E0 = gfield + (long long)T * D * M;
         float e[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int ix = 0; ix <= P; ix++)
-#pragma unroll
-          for (int iy = 0; iy <= P; iy++) {
-            const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
-            if (D == 3) {
-#pragma unroll
-              for (int iz = 0; iz <= P; iz++) {
-                const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
-                const float w = W[0][ix] * W[1][iy] * W[2][iz];
-#pragma unroll
-                for (int d = 0; d < D; d++) e[d] += E0[d * M + m] * w;
-              }
-            } else {
-              const float w = W[0][ix] * W[1][iy];
-#pragma unroll
-              for (int d = 0; d < D; d++) e[d] += E0[d * M + row] * w;
-            }
-          }
+        gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
 #pragma unroll
         for (int d = 0; d < D; d++) f[d] += e[d] * q;
       }
     }
+    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
+  }
+  // bonds
+  const int info = bond_info[i];
+  const int nb = info & 3;
+  for (int bb = 0; bb < nb; bb++) {
+    const int j = bond_nbr[3 * i + bb];
+    const int bt = (info >> (8 + 8 * bb)) & 0xff;
+    const float4 pj = pos_in[j];
+    const float xj[3] = {pj.x, pj.y, pj.z};
+    float dr[3], mdr2 = 0.f;
 #pragma unroll
-    for (int ix = 0; ix <= P; ix++)
-#pragma unroll
-      for (int iy = 0; iy <= P; iy++) {
-        const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
-        if (D == 3) {
-#pragma unroll
-          for (int iz = 0; iz <= P; iz++) {
-            const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
-            const float w = W[0][ix] * W[1][iy] * W[2][iz];
-#pragma unroll
-            for (int d = 0; d < D; d++) f[d] += G0[d * M + m] * w;
-          }
-        } else {
-          const float w = W[0][ix] * W[1][iy];
-#pragma unroll
-          for (int d = 0; d < D; d++) f[d] += G0[d * M + row] * w;
-        }
-      }
-    // bonds
-    const int info = bond_info[i];
-    const int nb = info & 3;
-    for (int bb = 0; bb < nb; bb++) {
-      const int j = bond_nbr[3 * i + bb];
-      const int bt = (info >> (8 + 8 * bb)) & 0xff;
-      const float4 pj = pos_in[j];
-      const float xj[3] = {pj.x, pj.y, pj.z};
-      float dr[3], mdr2 = 0.f;
-#pragma unroll
-      for (int d = 0; d < D; d++) {
-        dr[d] = x[d] - xj[d];
-        if (dr[d] > g.Lh[d]) dr[d] -= g.L[d];
-        else if (dr[d] < -g.Lh[d]) dr[d] += g.L[d];
-        mdr2 += dr[d] * dr[d];
-      }
-      float mf = 0.f;
-      if (mdr2 > 1.0E-4f) {
-        const float mdr = sqrtf(mdr2);
-        mf = 2.0f * ga.bond_k[bt] * (mdr - ga.bond_req[bt]) / mdr;
-      }
-#pragma unroll
-      for (int d = 0; d < D; d++) f[d] -= mf * dr[d];
+    for (int d = 0; d < D; d++) {
+      dr[d] = x[d] - xj[d];
+      if (dr[d] > g.Lh[d]) dr[d] -= g.L[d];
+      else if (dr[d] < -g.Lh[d]) dr[d] += g.L[d];
+      mdr2 += dr[d] * dr[d];
     }
-  } else {
-    atomicOr(status, ST_NONFINITE_POS);
+    float mf = 0.f;
+    if (mdr2 > 1.0E-4f) {
+      const float mdr = sqrtf(mdr2);
+      mf = 2.0f * ga.bond_k[bt] * (mdr - ga.bond_req[bt]) / mdr;
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) f[d] -= mf * dr[d];
   }
   const int bid = bead_id[i];
   if (f_out) {
@@ -306,7 +468,7 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ pos_i
   if (!INTEG) return;
   // integrators in input order (integrator.cu:24-39 is called for each in turn)
   const int mask = ga.type_mask[t];
-  float4 po = pos_io[i];  // x_{n-1} (GJF xo)
+  const float4 po = pos_io[i];  // x_{n-1} (GJF xo)
   float xo[3] = {po.x, po.y, po.z};
   float on[3] = {0.f, 0.f, 0.f};
   bool any_gjf = false;
@@ -364,29 +526,28 @@ __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ pos_i
 
 template <int D, int P>
 void launch_spread(tild_ctx* c) {
-  k_spread<D, P><<<nblk(c->ns, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->charge, c->ns, c->g, c->rho, c->T, c->C,
-                                                           c->d_status);
+  const size_t smem = sizeof(int) * (size_t)c->spread_cap;
+  cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_spread_tiled<D, P><<<nblk(c->ns, 256), 256, smem, c->stream>>>(c->pos[c->cur], c->charge, c->ns, c->g, c->rho_fx,
+                                                                    c->T, c->C, c->spread_cap, c->spread_kbits,
+                                                                    c->d_status);
+}
+
+template <int D, int P, bool I, bool X>
+void launch_gather_k(tild_ctx* c, const GArgs& ga, float* f_out) {
+  k_gather<D, P, I, X><<<nblk(c->ns, 256), 256, 0, c->stream>>>(
+      c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4, c->g,
+      c->T, c->C, ga, f_out, c->xorwow, c->ns, c->d_status);
 }
 
 template <int D, int P>
 void launch_gather(tild_ctx* c, const GArgs& ga, bool integ, float* f_out) {
-  const float4* pin = c->pos[c->cur];
-  float4* pio = c->pos[c->cur ^ 1];
-  const unsigned nb = nblk(c->ns, 256);
   const bool xw = c->cfg.rng == TILD_RNG_XORWOW;
   if (integ) {
-    if (xw)
-      k_gather<D, P, true, true><<<nb, 256, 0, c->stream>>>(pin, pio, c->noise, c->bead_id, c->bond_nbr, c->bond_info,
-                                                            c->charge, c->gfield, c->g, c->T, c->C, ga, f_out, c->xorwow,
-                                                            c->ns, c->d_status);
-    else
-      k_gather<D, P, true, false><<<nb, 256, 0, c->stream>>>(pin, pio, c->noise, c->bead_id, c->bond_nbr, c->bond_info,
-                                                             c->charge, c->gfield, c->g, c->T, c->C, ga, f_out,
-                                                             c->xorwow, c->ns, c->d_status);
+    if (xw) launch_gather_k<D, P, true, true>(c, ga, f_out);
+    else launch_gather_k<D, P, true, false>(c, ga, f_out);
   } else {
-    k_gather<D, P, false, false><<<nb, 256, 0, c->stream>>>(pin, pio, c->noise, c->bead_id, c->bond_nbr, c->bond_info,
-                                                            c->charge, c->gfield, c->g, c->T, c->C, ga, f_out,
-                                                            c->xorwow, c->ns, c->d_status);
+    launch_gather_k<D, P, false, false>(c, ga, f_out);
   }
 }
 
@@ -429,17 +590,24 @@ void launch_kmul(tild_ctx* c, const KArgs& ka) {
 }  // namespace
 
 int tild_run_spread(tild_ctx* c) {
-  tild_mark(c, STAGE_ZERO);
-  if (tild_check(c, cudaMemsetAsync(c->rho, 0, sizeof(float) * (size_t)(c->T + c->C) * c->g.M, c->stream), "zero rho"))
-    return TILD_ERR_CUDA;
+  // the fixed-point accumulator is all zeros here: it starts zeroed and k_fix_to_float clears it
   tild_mark(c, STAGE_SPREAD);
   if (c->D == 3) dispatch_p_spread<3>(c);
   else dispatch_p_spread<2>(c);
+  c->launches++;
+  tild_mark(c, STAGE_ZERO);
+  const long long n = (long long)(c->T + c->C) * c->g.M;
+  k_fix_to_float<<<nblk(n, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, n);
   c->launches++;
   return tild_check(c, cudaGetLastError(), "spread") ? TILD_ERR_CUDA : TILD_OK;
 }
 
 int tild_run_forces(tild_ctx* c, int64_t step, bool integrate, float* f_bead) {
+  if (integrate && c->sort_interval > 0 && step - 1 - c->last_sort_step >= c->sort_interval) {
+    tild_mark(c, STAGE_SORT);
+    int rs = tild_sort_beads(c);
+    if (rs) return rs;
+  }
   int rc = tild_run_spread(c);
   if (rc) return rc;
   tild_mark(c, STAGE_R2C);
@@ -489,6 +657,8 @@ int tild_run_forces(tild_ctx* c, int64_t step, bool integrate, float* f_bead) {
     ga.bond_req[b] = c->cfg.bond_req[b];
   }
   tild_mark(c, STAGE_GATHER);
+  k_interleave<<<nblk(c->g.M, 256), 256, 0, c->stream>>>(c->gfield, c->g4, c->T + c->C, c->D, c->g.M);
+  c->launches++;
   if (c->D == 3) dispatch_p_gather<3>(c, ga, integrate, f_bead);
   else dispatch_p_gather<2>(c, ga, integrate, f_bead);
   c->launches++;

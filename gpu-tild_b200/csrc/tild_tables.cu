@@ -232,6 +232,8 @@ int tild_build_tables(tild_ctx* c) {
   }
 
   const int nfft = (int)c->styles_k.size();
+  // per-direction real slabs start on 16-byte boundaries (cuFFT rejects a misaligned output)
+  const long long Mpad = (g.M + 1) / 2 * 2;
   double* ufull = nullptr;
   cufftDoubleComplex* zbuf = nullptr;
   cufftDoubleComplex* zbuf2 = nullptr;
@@ -243,7 +245,7 @@ int tild_build_tables(tild_ctx* c) {
     if (tild_check(c, cudaMalloc(&ufull, sizeof(double) * g.Mh), "alloc ufull") ||
         tild_check(c, cudaMalloc(&zbuf, sizeof(cufftDoubleComplex) * g.Mh), "alloc zbuf") ||
         tild_check(c, cudaMalloc(&zbuf2, sizeof(cufftDoubleComplex) * g.Mh), "alloc zbuf2") ||
-        tild_check(c, cudaMalloc(&freal, sizeof(double) * g.M * D), "alloc freal") ||
+        tild_check(c, cudaMalloc(&freal, sizeof(double) * Mpad * D), "alloc freal") ||
         tild_check(c, cudaMalloc(&vr, sizeof(double) * g.M), "alloc vr")) {
       rc = TILD_ERR_OOM;
     }
@@ -277,7 +279,7 @@ int tild_build_tables(tild_ctx* c) {
     for (int beta = 0; beta < D && rc == TILD_OK; beta++) {
       k_force_kernel<<<nblk(g.Mh, 256), 256, 0, st>>>(zbuf, ufull, g, D, beta);
       c->launches++;
-      if (tild_check_fft(c, cufftExecZ2D(pz2d, zbuf, freal + (long long)beta * g.M), "exec z2d")) rc = TILD_ERR_CUDA;
+      if (tild_check_fft(c, cufftExecZ2D(pz2d, zbuf, freal + (long long)beta * Mpad), "exec z2d")) rc = TILD_ERR_CUDA;
     }
     // virial kernels: FFT(dr_alpha f_beta) / M (InitializeVirial), times the 1/M that
     // CalcVirial applies to rho_k (pair_style.cu:277-279), stored on the half spectrum.
@@ -286,7 +288,7 @@ int tild_build_tables(tild_ctx* c) {
     for (int j = 0; j < c->nP && rc == TILD_OK; j++) {
       const int alpha = (D == 3) ? ab[j][0] : ab2[j][0];
       const int beta = (D == 3) ? ab[j][1] : ab2[j][1];
-      k_virial_real<<<nblk(g.M, 256), 256, 0, st>>>(vr, freal + (long long)beta * g.M, g, D, alpha);
+      k_virial_real<<<nblk(g.M, 256), 256, 0, st>>>(vr, freal + (long long)beta * Mpad, g, D, alpha);
       c->launches++;
       if (tild_check_fft(c, cufftExecD2Z(pd2z, vr, zbuf2), "exec d2z")) { rc = TILD_ERR_CUDA; break; }
       k_store_virk<<<nblk(g.Mh, 256), 256, 0, st>>>(c->virk + ((long long)s * c->nP + j) * g.Mh, zbuf2, g.Mh, invM * invM);
