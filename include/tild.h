@@ -221,6 +221,27 @@ int32_t tild_kernel_launches(tild_ctx* ctx, int64_t* count);
 /* Blocks until the context stream is idle; reports any device-side status flag. */
 int32_t tild_sync(tild_ctx* ctx);
 
+/* ---- allocation-free entry point ----------------------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device memory (code that
+ * runs inside another framework's allocator, or after device allocation has been closed): the
+ * bond energy and bond virial that host_bonds computes, from positions and topology the caller
+ * already holds on the device, with no cudaMalloc, cudaFree or allocating library call.  Its
+ * scratch is a fixed device array of TILD_NOALLOC_MAX_BLOCKS x 7 doubles (229 KB) that every GPU
+ * loading the library keeps until exit, so ns is limited to TILD_NOALLOC_MAX_BEADS; larger ns
+ * returns TILD_ERR_BAD_INPUT.  All calls share that array: calls that overlap on the GPU race.
+ * The first call on each device (that device current) looks the array up; make it before any
+ * stream capture.
+ *   d_x[ns*dim] float, d_n_bonds[ns], d_bonded_to[ns*3], d_bond_type[ns*3]: device arrays in the
+ *   read_config layout; box[3], bond_k[], bond_req[]: host arrays; d_out (device, FP64):
+ *   d_out[0] = bond energy, d_out[1..nP] = bond virial / (V * dim) (nP = 6 in 3D, 3 in 2D);
+ *   stream: a cudaStream_t or NULL.  The call is stream-ordered and does not synchronise. */
+#define TILD_NOALLOC_MAX_BLOCKS 4096
+#define TILD_NOALLOC_MAX_BEADS (TILD_NOALLOC_MAX_BLOCKS * 256)
+int32_t tild_bond_observables_noalloc(const float* d_x, const int32_t* d_n_bonds, const int32_t* d_bonded_to,
+                                      const int32_t* d_bond_type, int32_t ns, int32_t dim, const float* box,
+                                      int32_t n_bond_types, const float* bond_k, const float* bond_req,
+                                      double* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
