@@ -27,7 +27,6 @@ import shutil
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -36,6 +35,7 @@ sys.path[:0] = [os.path.join(ROOT, "gpu-tild_b200")]
 import numpy as np  # noqa: E402
 
 import tild  # noqa: E402
+import tild_dist  # noqa: E402
 import tild_systems as ts  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -134,48 +134,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus: int):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return None, 0, 0, 1
-    import torch
-    import torch.distributed as dist
-    rank = int(os.environ["RANK"])
-    local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
-    from datetime import timedelta
-    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    return dist, rank, local, ws
-
-
-def dist_max(dist, v: float) -> float:
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def dist_barrier(dist):
-    if dist is not None:
-        dist.barrier()
-
-
 # ------------------------------------------------------------------------------------------
 def run_ours(args):
-    dist, rank, local, ws = dist_setup(args.gpus)
+    grp = tild_dist.Group(backend="nccl")
+    rank, local, ws = grp.rank, grp.local, grp.world
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
-    launches0 = ctx.kernel_launches()
     ctx.step(args.warmup)
     ctx.sync()
-    dist_barrier(dist)
+    grp.barrier()
     with ClockSampler(local) as clk:
         l0 = ctx.kernel_launches()
         ms = ctx.time_steps(args.steps)
         launches = ctx.kernel_launches() - l0
-    ms = dist_max(dist, ms)
+    ms = grp.max(ms)
     clocks = clk.summary()
     per_rank = s.ns * args.steps
     value = per_rank * ws / (ms / 1e3)
@@ -204,7 +176,7 @@ def run_ours(args):
             obs_reads += 1
     xf, _, _ = ctx.get_state()
     e2e_s = time.perf_counter() - t0
-    e2e_s = dist_max(dist, e2e_s)
+    e2e_s = grp.max(e2e_s)
     obs_bytes = C_SIZEOF_OBS
     h2d = s.ns * s.dim * 4
     d2h = s.ns * s.dim * 4 + obs_reads * obs_bytes
@@ -232,8 +204,7 @@ def run_ours(args):
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(s, args)
     ctx.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    grp.close()
     if rank == 0:
         print(json.dumps(out))
 

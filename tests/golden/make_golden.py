@@ -4,8 +4,9 @@ Run in a checkout where the gpu-tild sources are available (default location bel
 box never needs them.  Outputs, next to this script:
   coacervate_config.npz   examples/Coacervate/input.data parsed as read_charge_config does
                           (positions FP32 via %f, types, charges, bond list)
-  coacervate_step0.json   the step-0 line of examples/Coacervate/data.dat and the input-script
-                          parameters of examples/Coacervate/input (the known-answer test)
+  coacervate_step0.json   the step-0 line of examples/Coacervate/data.dat, the input script
+                          examples/Coacervate/input and the runtime-parameter echo
+                          examples/Coacervate/NEED_A_NAME.input (the known-answer tests)
 """
 import json
 import os
@@ -36,6 +37,7 @@ def main():
         "script": {"Dim": 3, "Nx": [21, 21, 225], "pmeorder": 1, "charges": [0.43484, 1.0],
                    "gaussian": [[1, 1, 0.0003688, 1.0]], "bond": [1.5, 0.0], "delt": 0.005},
         "script_text": script,
+        "need_a_name_input": open(os.path.join(ex, "NEED_A_NAME.input")).read(),
     }
     with open(os.path.join(HERE, "coacervate_step0.json"), "w") as f:
         json.dump(gold, f, indent=1)
