@@ -19,13 +19,21 @@ int set_err(tild_ctx* c, int code, const char* msg) {
   return code;
 }
 
-// pack positions [ns][D] (bead order) into float4 slots with the type in .w
+// pack positions [ns][D] (bead order) of one system into float4 slots with the type in .w
 __global__ void k_pack_pos(const float* __restrict__ x, const int* __restrict__ types, const int* __restrict__ slot_of,
                            int ns, int D, float4* __restrict__ pos) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= ns) return;
   const float* xb = x + (long long)b * D;
   pos[slot_of[b]] = make_float4(xb[0], xb[1], D == 3 ? xb[2] : 0.f, __int_as_float(types[b] & 0xff));
+}
+
+__global__ void k_fill_padding(float4* __restrict__ p0, float4* __restrict__ p1, int n) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const float4 pad = make_float4(0.f, 0.f, 0.f, __int_as_float(kPadType));
+  p0[s] = pad;
+  p1[s] = pad;
 }
 
 __global__ void k_pack_noise(const float* __restrict__ src, const int* __restrict__ slot_of, int ns, int D,
@@ -36,10 +44,10 @@ __global__ void k_pack_noise(const float* __restrict__ src, const int* __restric
   for (int d = 0; d < 3; d++) noise[3 * (long long)s + d] = (src && d < D) ? src[(long long)b * D + d] : 0.f;
 }
 
-__global__ void k_unpack_pos(const float4* __restrict__ pos, const int* __restrict__ bead_id, int ns, int D,
+__global__ void k_unpack_pos(const float4* __restrict__ pos, const int* __restrict__ bead_id, int n, int D,
                              float* __restrict__ x) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+  if (s >= n || bead_id[s] < 0) return;
   const float4 p = pos[s];
   float* xb = x + (long long)bead_id[s] * D;
   xb[0] = p.x;
@@ -47,16 +55,16 @@ __global__ void k_unpack_pos(const float4* __restrict__ pos, const int* __restri
   if (D == 3) xb[2] = p.z;
 }
 
-__global__ void k_unpack_noise(const float* __restrict__ noise, const int* __restrict__ bead_id, int ns, int D,
+__global__ void k_unpack_noise(const float* __restrict__ noise, const int* __restrict__ bead_id, int n, int D,
                                float* __restrict__ out) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+  if (s >= n || bead_id[s] < 0) return;
   for (int d = 0; d < D; d++) out[(long long)bead_id[s] * D + d] = noise[3 * (long long)s + d];
 }
 
-__global__ void k_init_xorwow(curandStateXORWOW_t* st, const int* __restrict__ bead_id, int ns, unsigned int seed) {
+__global__ void k_init_xorwow(curandStateXORWOW_t* st, const int* __restrict__ bead_id, int n, unsigned int seed) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+  if (s >= n || bead_id[s] < 0) return;
   // init_dev_rng (cuda_random_posits.cu:22-30): curand_init(seed, bead, 0)
   curand_init(seed, (unsigned long long)bead_id[s], 0, &st[s]);
 }
@@ -76,16 +84,19 @@ int dalloc(tild_ctx* c, T** p, size_t n, const char* what) {
 
 void free_all(tild_ctx* c) {
   void* ptrs[] = {c->pos[0], c->pos[1], c->noise, c->bead_id, c->slot_of, c->bond_nbr, c->bond_info, c->charge,
-                  c->bondk_dev, c->bondr_dev, c->types_dev, c->xorwow, c->rho, c->rhok, c->gk, c->gfield, c->utab,
-                  c->ctab, c->virk, c->frfield, c->rho_fx, c->g4, c->kd, c->kk, c->red, c->xfer, c->d_status};
+                  c->types_dev, c->xorwow, c->rho, c->rhok, c->gk, c->gfield, c->utab, c->ctab, c->virk, c->frfield,
+                  c->rho_fx, c->g4, c->kd, c->kk, c->red, c->xfer, c->d_status, c->d_sys, c->cta_bead, c->cta_spec,
+                  c->cta_grid};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  for (int i = 0; i < TILD_MAX_COMPUTES; i++)
-    if (c->sk[i]) cudaFree(c->sk[i]);
-  if (c->plans) {
-    cufftDestroy(c->plan_r2c);
-    cufftDestroy(c->plan_c2r);
-  }
+  for (SysHost& h : c->sys)
+    for (int i = 0; i < TILD_MAX_COMPUTES; i++)
+      if (h.sk[i]) cudaFree(h.sk[i]);
+  for (Bucket& b : c->buckets)
+    if (b.planned) {
+      cufftDestroy(b.r2c);
+      cufftDestroy(b.c2r);
+    }
   tild_sort_free(c);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -139,7 +150,495 @@ int validate(const tild_config* cfg, std::string& why) {
   return TILD_OK;
 }
 
+// Fixed-point scale of the shared-memory spread: 256 beads x the largest product of stencil
+// weights (times the largest |q| on the charge channel) must stay below 2^31.
+int spread_kbits(int P, int D, double gvol, double qmax) {
+  double wmax = 0.0;
+  for (int k = 0; k <= 1000; k++) {
+    const double sx = -0.5 + k / 1000.0;
+    double W[5];
+    const double sx2 = sx * sx;
+    double sx3, sx4;
+    if (P == 0) { W[0] = 1; }
+    else if (P == 1) { W[0] = 0.5 - sx; W[1] = 0.5 + sx; }
+    else if (P == 2) { W[0] = 0.125 - 0.5 * sx + 0.5 * sx2; W[1] = 0.75 - sx2; W[2] = 0.125 + 0.5 * sx + 0.5 * sx2; }
+    else if (P == 3) { sx3 = sx2 * sx; W[0] = (1 - 6 * sx + 12 * sx2 - 8 * sx3) / 48; W[1] = (23 - 30 * sx - 12 * sx2 + 24 * sx3) / 48;
+                       W[2] = (23 + 30 * sx - 12 * sx2 - 24 * sx3) / 48; W[3] = (1 + 6 * sx + 12 * sx2 + 8 * sx3) / 48; }
+    else { sx3 = sx2 * sx2; sx4 = sx2 * sx2; W[0] = (1 - 8 * sx + 24 * sx2 - 32 * sx3 + 16 * sx4) / 384;
+           W[1] = (19 - 44 * sx + 24 * sx2 + 16 * sx3 - 16 * sx4) / 96; W[2] = (115 - 120 * sx2 + 48 * sx4) / 192;
+           W[3] = (19 + 44 * sx + 24 * sx2 - 16 * sx3 - 16 * sx4) / 96; W[4] = (1 + 8 * sx + 24 * sx2 + 32 * sx3 + 16 * sx4) / 384; }
+    for (int a = 0; a <= P; a++) wmax = std::max(wmax, std::fabs(W[a]));
+  }
+  const double bound = 256.0 * std::pow(wmax * 1.05, D) / gvol * std::max(qmax, 1.0);
+  int k = 0;
+  while (k < 31 && bound * std::ldexp(1.0, k + 1) < 2147483647.0) k++;
+  return k;
+}
+
+int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
+  std::string why;
+  for (int s = 0; s < nsys; s++) {
+    int v = validate(&cfgs[s], why);
+    if (v) {
+      c->err = "system " + std::to_string(s) + ": " + why;
+      return v;
+    }
+    if (cfgs[s].dim != cfgs[0].dim || cfgs[s].pmeorder != cfgs[0].pmeorder || cfgs[s].rng != cfgs[0].rng) {
+      c->err = "systems of one batch must share dim, pmeorder and rng";
+      return TILD_ERR_UNSUPPORTED;
+    }
+  }
+  c->device = device;
+  if (tild_check(c, cudaSetDevice(device), "cudaSetDevice")) return TILD_ERR_CUDA;
+  if (tild_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) return TILD_ERR_CUDA;
+  c->D = cfgs[0].dim;
+  c->P = cfgs[0].pmeorder;
+  c->rng = cfgs[0].rng;
+  c->nsys = nsys;
+  c->sys.resize(nsys);
+  c->h_sys.assign(nsys, SysDev());
+  memset(c->h_sys.data(), 0, sizeof(SysDev) * nsys);
+  c->sort_interval = cfgs[0].sort_interval == 0 ? 16 : (cfgs[0].sort_interval < 0 ? 0 : cfgs[0].sort_interval);
+  c->steps_since_sort = c->sort_interval;
+  c->spread_cap = 12288;
+  long long slots = 0, beads = 0, utab = 0, virk = 0, ctab = 0, kd = 0, fr = 0;
+  // buckets by grid shape (order of first appearance)
+  for (int s = 0; s < nsys; s++) {
+    const tild_config& cfg = cfgs[s];
+    SysHost& h = c->sys[s];
+    h.cfg = cfg;
+    h.D = cfg.dim;
+    h.T = cfg.ntypes;
+    h.C = cfg.do_charges ? 1 : 0;
+    h.ns = cfg.ns;
+    h.p = cfg.pmeorder;
+    h.nP = (h.D == 2) ? 3 : 6;
+    Geom& g = h.g;
+    g.M = 1;
+    h.S = 1;
+    float gv = 1.0f;
+    for (int d = 0; d < 3; d++) {
+      g.nx[d] = (d < h.D) ? cfg.nx[d] : 1;
+      g.L[d] = (d < h.D) ? cfg.box[d] : 1.0f;
+      g.Lh[d] = 0.5f * g.L[d];
+      g.dx[d] = g.L[d] / (float)g.nx[d];
+    }
+    h.dV = 1.0;
+    h.V = 1.0;
+    for (int d = 0; d < h.D; d++) {
+      gv *= g.dx[d];
+      g.M *= g.nx[d];
+      h.S *= (h.p + 1);
+      h.dV *= (double)g.dx[d];
+      h.V *= (double)g.L[d];
+    }
+    g.gvol = gv;
+    g.nxh = g.nx[0] / 2 + 1;
+    g.Mh = g.M / g.nx[0] * g.nxh;
+    h.ns_pad = (h.ns + kTile - 1) / kTile * kTile;
+    h.slot0 = (int)slots;
+    h.bead0 = (int)beads;
+    slots += h.ns_pad;
+    beads += h.ns;
+    SysDev& d = c->h_sys[s];
+    int nfft = 0;
+    for (int i = 0; i < cfg.n_styles; i++) {
+      const tild_pair_style& ps = cfg.styles[i];
+      if (ps.style == TILD_STYLE_FIELDPHASE) {
+        FieldK f;
+        f.sys = s;
+        f.a = ps.type1;
+        f.b = ps.type2;
+        f.cfg_index = i;
+        f.fr0 = fr;
+        fr += (long long)h.D * g.M;
+        c->fields.push_back(f);
+      } else {
+        d.sa[nfft] = ps.type1;
+        d.sb[nfft] = ps.type2;
+        d.sramp[nfft] = ps.ramp;
+        d.sAi[nfft] = ps.prefactor;
+        d.sAf[nfft] = ps.final_prefactor;
+        d.suk0[nfft] = 1.0f;
+        h.fft_cfg.push_back(i);
+        nfft++;
+      }
+    }
+    for (int t = 0; t < h.T; t++) {
+      int m = 0;
+      for (int k = 0; k < cfg.n_integrators; k++)
+        if (cfg.integrators[k].group_type < 0 || cfg.integrators[k].group_type == t) m |= 1 << k;
+      h.type_integ_mask[t] = m;
+    }
+    h.utab0 = utab;
+    utab += (long long)nfft * g.Mh;
+    h.virk0 = virk;
+    virk += (long long)nfft * h.nP * g.Mh;
+    h.ctab0 = ctab;
+    ctab += (long long)h.C * g.Mh;
+    h.kd0 = kd;
+    kd += g.nx[0] + g.nx[1] + g.nx[2];
+    c->maxT = std::max(c->maxT, h.T);
+    c->any_charges |= h.C != 0;
+    int bi = -1;
+    for (size_t k = 0; k < c->buckets.size(); k++)
+      if (c->buckets[k].nx[0] == g.nx[0] && c->buckets[k].nx[1] == g.nx[1] && c->buckets[k].nx[2] == g.nx[2]) bi = (int)k;
+    if (bi < 0) {
+      Bucket b;
+      for (int q = 0; q < 3; q++) b.nx[q] = g.nx[q];
+      c->buckets.push_back(b);
+      bi = (int)c->buckets.size() - 1;
+    }
+    c->buckets[bi].systems.push_back(s);
+    h.bucket = bi;
+    // device descriptor
+    d.g = g;
+    d.T = h.T;
+    d.C = h.C;
+    d.nfft = nfft;
+    d.slot0 = h.slot0;
+    d.ns = h.ns;
+    d.ns_pad = h.ns_pad;
+    d.bead0 = h.bead0;
+    d.active = 1;
+    d.utab0 = h.utab0;
+    d.ctab0 = h.ctab0;
+    d.kd0 = h.kd0;
+    d.step = 0;
+    d.max_steps = cfg.max_steps;
+    d.seed = cfg.seed;
+    d.delt = cfg.delt;
+    d.noise_mag = cfg.noise_mag;
+    d.n_integ = cfg.n_integrators;
+    for (int k = 0; k < cfg.n_integrators; k++) d.integ_kind[k] = cfg.integrators[k].kind;
+    for (int t = 0; t < h.T; t++) {
+      d.type_mask[t] = h.type_integ_mask[t];
+      d.mass[t] = cfg.mass[t];
+      d.diff[t] = cfg.diff[t];
+    }
+    for (int b = 0; b < cfg.n_bond_types; b++) {
+      d.bond_k[b] = cfg.bond_k[b];
+      d.bond_req[b] = cfg.bond_req[b];
+    }
+    h.kbits = spread_kbits(h.p, h.D, g.gvol, 1.0);
+    d.kbits = h.kbits;
+  }
+  // channel layout: bucket by bucket so each bucket is one batched transform
+  long long grid = 0, spec = 0;
+  for (Bucket& b : c->buckets) {
+    b.grid0 = grid;
+    b.spec0 = spec;
+    b.channels = 0;
+    for (int s : b.systems) {
+      SysHost& h = c->sys[s];
+      h.grid0 = grid;
+      h.spec0 = spec;
+      c->h_sys[s].grid0 = grid;
+      c->h_sys[s].spec0 = spec;
+      grid += (long long)(h.T + h.C) * h.g.M;
+      spec += (long long)(h.T + h.C) * h.g.Mh;
+      b.channels += h.T + h.C;
+    }
+  }
+  c->grid_total = grid;
+  c->spec_total = spec;
+  c->nslots = (int)slots;
+  c->nbeads = (int)beads;
+  // CTA -> system lookup tables (grid and spectrum tables carry each system's first block after them)
+  std::vector<int> tb, tspec, tgrid, bspec(nsys), bgrid(nsys);
+  for (int s = 0; s < nsys; s++) {
+    const SysHost& h = c->sys[s];
+    for (int k = 0; k < h.ns_pad / kTile; k++) tb.push_back(s);
+    bspec[s] = (int)tspec.size();
+    for (long long k = 0; k < (h.g.Mh + 255) / 256; k++) tspec.push_back(s);
+    bgrid[s] = (int)tgrid.size();
+    for (long long k = 0; k < (h.g.M + 255) / 256; k++) tgrid.push_back(s);
+  }
+  c->n_cta_bead = (int)tb.size();
+  c->n_cta_spec = (int)tspec.size();
+  c->n_cta_grid = (int)tgrid.size();
+  tspec.insert(tspec.end(), bspec.begin(), bspec.end());
+  tgrid.insert(tgrid.end(), bgrid.begin(), bgrid.end());
+  int maxns = 1;
+  for (const SysHost& h : c->sys) maxns = std::max(maxns, h.ns);
+  const size_t NS = c->nslots;
+  int rc = TILD_OK;
+  rc = rc ? rc : dalloc(c, &c->pos[0], NS, "positions");
+  rc = rc ? rc : dalloc(c, &c->pos[1], NS, "positions");
+  rc = rc ? rc : dalloc(c, &c->noise, NS * 3, "noise");
+  rc = rc ? rc : dalloc(c, &c->bead_id, NS, "bead ids");
+  rc = rc ? rc : dalloc(c, &c->slot_of, (size_t)c->nbeads, "slots");
+  rc = rc ? rc : dalloc(c, &c->bond_nbr, NS * 3, "bonds");
+  rc = rc ? rc : dalloc(c, &c->bond_info, NS, "bonds");
+  rc = rc ? rc : dalloc(c, &c->types_dev, (size_t)c->nbeads, "types");
+  if (c->any_charges) rc = rc ? rc : dalloc(c, &c->charge, NS, "charges");
+  rc = rc ? rc : dalloc(c, &c->rho, (size_t)grid, "densities");
+  rc = rc ? rc : dalloc(c, &c->rho_fx, (size_t)grid, "density accumulator");
+  rc = rc ? rc : dalloc(c, &c->rhok, (size_t)spec, "density spectra");
+  rc = rc ? rc : dalloc(c, &c->gk, (size_t)spec * c->D, "force spectra");
+  rc = rc ? rc : dalloc(c, &c->gfield, (size_t)grid * c->D, "force fields");
+  rc = rc ? rc : dalloc(c, &c->g4, (size_t)grid, "interleaved force fields");
+  rc = rc ? rc : dalloc(c, &c->utab, (size_t)utab, "multiplier tables");
+  rc = rc ? rc : dalloc(c, &c->virk, (size_t)virk, "virial tables");
+  if (ctab) rc = rc ? rc : dalloc(c, &c->ctab, (size_t)ctab, "charge table");
+  if (fr) rc = rc ? rc : dalloc(c, &c->frfield, (size_t)fr, "fieldphase fields");
+  rc = rc ? rc : dalloc(c, &c->kd, (size_t)kd, "k vectors");
+  rc = rc ? rc : dalloc(c, &c->kk, (size_t)kd, "k vectors");
+  rc = rc ? rc : dalloc(c, &c->xfer, (size_t)maxns * 3, "transfer buffer");
+  rc = rc ? rc : dalloc(c, &c->d_status, 1, "status");
+  rc = rc ? rc : dalloc(c, &c->d_sys, (size_t)nsys, "system descriptors");
+  rc = rc ? rc : dalloc(c, &c->cta_bead, tb.size(), "lookup");
+  rc = rc ? rc : dalloc(c, &c->cta_spec, tspec.size(), "lookup");
+  rc = rc ? rc : dalloc(c, &c->cta_grid, tgrid.size(), "lookup");
+  if (c->rng == TILD_RNG_XORWOW) rc = rc ? rc : dalloc(c, &c->xorwow, NS, "xorwow states");
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  cudaMemsetAsync(c->d_status, 0, sizeof(int), st);
+  cudaMemsetAsync(c->rho_fx, 0, sizeof(unsigned long long) * grid, st);
+  cudaMemsetAsync(c->noise, 0, sizeof(float) * NS * 3, st);
+  cudaMemsetAsync(c->bond_nbr, 0, sizeof(int) * NS * 3, st);
+  cudaMemsetAsync(c->bond_info, 0, sizeof(int) * NS, st);
+  cudaMemsetAsync(c->bead_id, 0xff, sizeof(int) * NS, st);
+  if (c->charge) cudaMemsetAsync(c->charge, 0, sizeof(float) * NS, st);
+  k_fill_padding<<<nblk(NS, 256), 256, 0, st>>>(c->pos[0], c->pos[1], (int)NS);
+  c->launches++;
+  cudaMemcpyAsync(c->cta_bead, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->cta_spec, tspec.data(), tspec.size() * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->cta_grid, tgrid.data(), tgrid.size() * 4, cudaMemcpyHostToDevice, st);
+  if (tild_check(c, cudaStreamSynchronize(st), "init")) return TILD_ERR_CUDA;
+  // batched cuFFT plans, one pair per grid shape
+  for (Bucket& b : c->buckets) {
+    int n[3];
+    if (c->D == 3) { n[0] = b.nx[2]; n[1] = b.nx[1]; n[2] = b.nx[0]; }
+    else { n[0] = b.nx[1]; n[1] = b.nx[0]; }
+    if (tild_check_fft(c, cufftPlanMany(&b.r2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, b.channels), "plan R2C"))
+      return TILD_ERR_CUDA;
+    if (tild_check_fft(c, cufftPlanMany(&b.c2r, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, b.channels * c->D), "plan C2R")) {
+      cufftDestroy(b.r2c);
+      return TILD_ERR_CUDA;
+    }
+    b.planned = true;
+    if (tild_check_fft(c, cufftSetStream(b.r2c, st), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, st), "plan stream"))
+      return TILD_ERR_CUDA;
+  }
+  for (int s = 0; s < nsys && !rc; s++) rc = tild_build_tables(c, s);
+  if (rc) return rc;
+  if (c->sort_interval > 0) {
+    rc = tild_sort_alloc(c);
+    if (rc) return rc;
+  }
+  return tild_upload_sys(c);
+}
+
+int check_sys(tild_ctx* c, int s) {
+  if (!c || s < 0 || s >= c->nsys) return TILD_ERR_BAD_INPUT;
+  return TILD_OK;
+}
+
+int sys_set_topology(tild_ctx* c, int s, const int32_t* types, const float* charges, const int32_t* n_bonds,
+                     const int32_t* bonded_to, const int32_t* bond_type) {
+  if (check_sys(c, s) || !types) return TILD_ERR_BAD_INPUT;
+  SysHost& h = c->sys[s];
+  if (h.C && !charges) return set_err(c, TILD_ERR_BAD_INPUT, "charges required when do_charges is set");
+  cudaSetDevice(c->device);
+  const int ns = h.ns, np = h.ns_pad;
+  std::vector<int> nbr(3 * (size_t)np, 0), info(np, 0), bid(np, -1), slot_of(ns);
+  std::vector<float> q;
+  if (c->charge) q.assign(np, 0.f);
+  double qmax = 1.0;
+  for (int b = 0; b < ns; b++) {
+    if (types[b] < 0 || types[b] >= h.T) return set_err(c, TILD_ERR_BAD_INPUT, "bead type out of range");
+    int nb = n_bonds ? n_bonds[b] : 0;
+    if (nb < 0 || nb > TILD_MAX_BONDS) return set_err(c, TILD_ERR_BAD_INPUT, "more than MAX_BONDS (3) bonds on a bead");
+    int in = nb;
+    for (int k = 0; k < nb; k++) {
+      const int j = bonded_to[3 * (size_t)b + k], bt = bond_type[3 * (size_t)b + k];
+      if (j < 0 || j >= ns) return set_err(c, TILD_ERR_BAD_INPUT, "bond partner out of range");
+      if (bt < 0 || bt >= h.cfg.n_bond_types) return set_err(c, TILD_ERR_BAD_INPUT, "bond type out of range");
+      nbr[3 * (size_t)b + k] = h.slot0 + j;
+      in |= bt << (8 + 8 * k);
+    }
+    info[b] = in;
+    bid[b] = b;
+    slot_of[b] = h.slot0 + b;
+    if (h.C) {
+      q[b] = charges[b];
+      qmax = std::max(qmax, (double)std::fabs(charges[b]));
+    }
+  }
+  cudaStream_t st = c->stream;
+  if (tild_check(c, cudaMemcpyAsync(c->bond_nbr + 3 * (size_t)h.slot0, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, st), "bonds") ||
+      tild_check(c, cudaMemcpyAsync(c->bond_info + h.slot0, info.data(), info.size() * 4, cudaMemcpyHostToDevice, st), "bonds") ||
+      tild_check(c, cudaMemcpyAsync(c->bead_id + h.slot0, bid.data(), bid.size() * 4, cudaMemcpyHostToDevice, st), "ids") ||
+      tild_check(c, cudaMemcpyAsync(c->slot_of + h.bead0, slot_of.data(), slot_of.size() * 4, cudaMemcpyHostToDevice, st), "slots") ||
+      tild_check(c, cudaMemcpyAsync(c->types_dev + h.bead0, types, (size_t)ns * 4, cudaMemcpyHostToDevice, st), "types") ||
+      (c->charge && tild_check(c, cudaMemcpyAsync(c->charge + h.slot0, q.data(), (size_t)np * 4, cudaMemcpyHostToDevice, st), "charges")))
+    return TILD_ERR_CUDA;
+  k_fill_padding<<<nblk(np, 256), 256, 0, st>>>(c->pos[0] + h.slot0, c->pos[1] + h.slot0, np);
+  c->launches++;
+  if (tild_check(c, cudaStreamSynchronize(st), "sync topology")) return TILD_ERR_CUDA;
+  h.kbits = spread_kbits(h.p, h.D, h.g.gvol, qmax);
+  c->h_sys[s].kbits = h.kbits;
+  h.topo_set = true;
+  h.state_set = false;
+  h.have_forces = false;
+  return tild_upload_sys(c);
+}
+
+int sys_set_state(tild_ctx* c, int s, const float* x, const float* xo, const float* prev_noise) {
+  if (check_sys(c, s) || !x) return TILD_ERR_BAD_INPUT;
+  SysHost& h = c->sys[s];
+  if (!h.topo_set) return set_err(c, TILD_ERR_STATE, "tild_set_topology must come before tild_set_state");
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)h.ns * h.D;
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(x[i])) return set_err(c, TILD_ERR_NAN, "non-finite position in tild_set_state");
+  const unsigned nb = nblk(h.ns, 256);
+  cudaStream_t st = c->stream;
+  const int* so = c->slot_of + h.bead0;
+  const int* ty = c->types_dev + h.bead0;
+  if (tild_check(c, cudaMemcpyAsync(c->xfer, x, n * 4, cudaMemcpyHostToDevice, st), "upload x")) return TILD_ERR_CUDA;
+  k_pack_pos<<<nb, 256, 0, st>>>(c->xfer, ty, so, h.ns, h.D, c->pos[c->cur]);
+  // x_{n-1}: xo when given, else x (send_3n_to_device copies x into xo, device_comm_utils.cu:15-16)
+  if (xo && tild_check(c, cudaMemcpyAsync(c->xfer, xo, n * 4, cudaMemcpyHostToDevice, st), "upload xo"))
+    return TILD_ERR_CUDA;
+  k_pack_pos<<<nb, 256, 0, st>>>(c->xfer, ty, so, h.ns, h.D, c->pos[c->cur ^ 1]);
+  if (prev_noise && tild_check(c, cudaMemcpyAsync(c->xfer, prev_noise, n * 4, cudaMemcpyHostToDevice, st), "upload noise"))
+    return TILD_ERR_CUDA;
+  k_pack_noise<<<nb, 256, 0, st>>>(prev_noise ? c->xfer : nullptr, so, h.ns, h.D, c->noise);
+  c->launches += 3;
+  if (c->xorwow) {
+    k_init_xorwow<<<nblk(h.ns_pad, 256), 256, 0, st>>>(c->xorwow + h.slot0, c->bead_id + h.slot0, h.ns_pad,
+                                                        (unsigned int)h.cfg.seed);
+    c->launches++;
+  }
+  if (tild_check(c, cudaStreamSynchronize(st), "set state")) return TILD_ERR_CUDA;
+  c->steps_since_sort = c->sort_interval;  // sort before the next step
+  h.state_set = true;
+  h.have_forces = false;
+  return TILD_OK;
+}
+
+int sys_get_state(tild_ctx* c, int s, float* x, float* xo, float* prev_noise) {
+  if (check_sys(c, s)) return TILD_ERR_BAD_INPUT;
+  SysHost& h = c->sys[s];
+  if (!h.state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)h.ns * h.D;
+  const unsigned nb = nblk(h.ns_pad, 256);
+  float* outs[3] = {x, xo, prev_noise};
+  for (int k = 0; k < 3; k++) {
+    if (!outs[k]) continue;
+    if (k < 2)
+      k_unpack_pos<<<nb, 256, 0, c->stream>>>(c->pos[k == 0 ? c->cur : c->cur ^ 1] + h.slot0, c->bead_id + h.slot0,
+                                               h.ns_pad, h.D, c->xfer);
+    else
+      k_unpack_noise<<<nb, 256, 0, c->stream>>>(c->noise + 3 * (size_t)h.slot0, c->bead_id + h.slot0, h.ns_pad, h.D,
+                                                 c->xfer);
+    c->launches++;
+    if (tild_check(c, cudaMemcpyAsync(outs[k], c->xfer, n * 4, cudaMemcpyDeviceToHost, c->stream), "download") ||
+        tild_check(c, cudaStreamSynchronize(c->stream), "sync download"))
+      return TILD_ERR_CUDA;
+  }
+  return TILD_OK;
+}
+
+bool all_ready(tild_ctx* c) {
+  for (const SysHost& h : c->sys)
+    if (h.active && !h.state_set) return false;
+  return true;
+}
+
+int engine_step(tild_ctx* c, int nsteps) {
+  if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "every active system needs tild_set_state before stepping");
+  cudaSetDevice(c->device);
+  for (int k = 0; k < nsteps; k++) {
+    int rc = tild_run_forces(c, true, nullptr, -1);
+    if (rc) return rc;
+  }
+  return tild_poll_status(c);
+}
+
+int sys_forces(tild_ctx* c, int s, float* f) {
+  if (check_sys(c, s)) return TILD_ERR_BAD_INPUT;
+  if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "tild_set_state must come before tild_forces");
+  cudaSetDevice(c->device);
+  int rc = tild_run_forces(c, false, f ? c->xfer : nullptr, s);
+  if (rc) return rc;
+  rc = tild_poll_status(c);
+  if (rc) return rc;
+  if (f) {
+    const SysHost& h = c->sys[s];
+    if (tild_check(c, cudaMemcpyAsync(f, c->xfer, (size_t)h.ns * h.D * 4, cudaMemcpyDeviceToHost, c->stream), "download f") ||
+        tild_check(c, cudaStreamSynchronize(c->stream), "sync f"))
+      return TILD_ERR_CUDA;
+  }
+  return TILD_OK;
+}
+
+int sys_observables(tild_ctx* c, int s, tild_obs* o) {
+  if (check_sys(c, s) || !o) return TILD_ERR_BAD_INPUT;
+  if (!c->sys[s].state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  cudaSetDevice(c->device);
+  if (!c->sys[s].have_forces) {
+    int rc = tild_run_forces(c, false, nullptr, -1);
+    if (rc) return rc;
+  }
+  int rc = tild_obs_compute(c, s, o);
+  if (rc) return rc;
+  if (!std::isfinite(o->upe)) return set_err(c, TILD_ERR_NAN, "non-finite energy");
+  return tild_poll_status(c);
+}
+
+int sys_density(tild_ctx* c, int s, float* rho) {
+  if (check_sys(c, s) || !rho) return TILD_ERR_BAD_INPUT;
+  const SysHost& h = c->sys[s];
+  if (!h.have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
+  cudaSetDevice(c->device);
+  if (tild_check(c, cudaMemcpyAsync(rho, c->rho + h.grid0, sizeof(float) * (size_t)(h.T + h.C) * h.g.M, cudaMemcpyDeviceToHost, c->stream), "download rho") ||
+      tild_check(c, cudaStreamSynchronize(c->stream), "sync rho"))
+    return TILD_ERR_CUDA;
+  return TILD_OK;
+}
+
+int sys_set_step(tild_ctx* c, int s, int64_t step) {
+  if (check_sys(c, s) || step < 0) return TILD_ERR_BAD_INPUT;
+  c->sys[s].step = step;
+  c->h_sys[s].step = step;
+  return tild_upload_sys(c);
+}
+
+int engine_time(tild_ctx* c, int nsteps, double* ms) {
+  if (!c || !ms || nsteps < 0) return TILD_ERR_BAD_INPUT;
+  if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "no state");
+  cudaSetDevice(c->device);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c->stream);
+  int rc = TILD_OK;
+  for (int k = 0; k < nsteps && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc ? rc : tild_poll_status(c);
+}
+
 }  // namespace
+
+struct tild_batch : public tild_ctx {};
+
+int tild_upload_sys(tild_ctx* c) {
+  for (int s = 0; s < c->nsys; s++) c->h_sys[s].active = c->sys[s].active ? 1 : 0;
+  if (tild_check(c, cudaMemcpyAsync(c->d_sys, c->h_sys.data(), sizeof(SysDev) * c->nsys, cudaMemcpyHostToDevice, c->stream), "upload descriptors") ||
+      tild_check(c, cudaStreamSynchronize(c->stream), "sync descriptors"))
+    return TILD_ERR_CUDA;
+  return TILD_OK;
+}
 
 int tild_check(tild_ctx* c, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return 0;
@@ -190,158 +689,11 @@ const char* tild_status_string(int32_t s) {
 
 const char* tild_last_error(const tild_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
-  if (!cfg || !out) return TILD_ERR_BAD_INPUT;
+static int create_common(const tild_config* cfgs, int nsys, int device, tild_batch** out) {
+  if (!cfgs || !out || nsys < 1) return TILD_ERR_BAD_INPUT;
   *out = nullptr;
-  std::string why;
-  int v = validate(cfg, why);
-  if (v) {
-    fprintf(stderr, "tild_create: %s\n", why.c_str());
-    return v;
-  }
-  tild_ctx* c = new tild_ctx();
-  c->cfg = *cfg;
-  c->device = device;
-  if (tild_check(c, cudaSetDevice(device), "cudaSetDevice")) {
-    fprintf(stderr, "tild_create: %s\n", c->err.c_str());
-    delete c;
-    return TILD_ERR_CUDA;
-  }
-  if (tild_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) {
-    delete c;
-    return TILD_ERR_CUDA;
-  }
-  c->D = cfg->dim;
-  c->T = cfg->ntypes;
-  c->C = cfg->do_charges ? 1 : 0;
-  c->ns = cfg->ns;
-  c->p = cfg->pmeorder;
-  c->nP = (c->D == 2) ? 3 : 6;
-  c->max_steps = cfg->max_steps;
-  Geom& g = c->g;
-  g.M = 1;
-  c->S = 1;
-  float gv = 1.0f;
-  for (int d = 0; d < 3; d++) {
-    g.nx[d] = (d < c->D) ? cfg->nx[d] : 1;
-    g.L[d] = (d < c->D) ? cfg->box[d] : 1.0f;
-    g.Lh[d] = 0.5f * g.L[d];
-    g.dx[d] = g.L[d] / (float)g.nx[d];
-  }
-  c->dV = 1.0;
-  c->V = 1.0;
-  for (int d = 0; d < c->D; d++) {
-    gv *= g.dx[d];
-    g.M *= g.nx[d];
-    c->S *= (c->p + 1);
-    c->dV *= (double)g.dx[d];
-    c->V *= (double)g.L[d];
-  }
-  g.gvol = gv;
-  g.nxh = g.nx[0] / 2 + 1;
-  g.Mh = g.M / g.nx[0] * g.nxh;
-
-  // style bookkeeping: FFT styles get a table slot, fieldphases a static field
-  c->fft_style_index.assign(cfg->n_styles, -1);
-  for (int i = 0; i < cfg->n_styles; i++) {
-    const tild_pair_style& s = cfg->styles[i];
-    if (s.style == TILD_STYLE_FIELDPHASE) {
-      FieldK f;
-      f.a = s.type1;
-      f.b = s.type2;
-      f.slot = i;
-      c->fields.push_back(f);
-    } else {
-      StyleK k;
-      k.a = s.type1;
-      k.b = s.type2;
-      k.ramp = s.ramp;
-      k.Ai = s.prefactor;
-      k.Af = s.final_prefactor;
-      k.uk0 = 1.0f;
-      c->fft_style_index[i] = (int)c->styles_k.size();
-      c->fft_style_cfg.push_back(i);
-      c->styles_k.push_back(k);
-    }
-  }
-  for (int t = 0; t < c->T; t++) {
-    int m = 0;
-    for (int k = 0; k < cfg->n_integrators; k++)
-      if (cfg->integrators[k].group_type < 0 || cfg->integrators[k].group_type == t) m |= 1 << k;
-    c->type_integ_mask[t] = m;
-  }
-
-  const size_t ns = c->ns, M = g.M, Mh = g.Mh;
-  c->spread_cap = 12288;
-  const size_t nch = c->T + c->C;
-  const size_t nfft = c->styles_k.size();
-  int rc = TILD_OK;
-  rc = rc ? rc : dalloc(c, &c->pos[0], ns, "positions");
-  rc = rc ? rc : dalloc(c, &c->pos[1], ns, "positions");
-  rc = rc ? rc : dalloc(c, &c->noise, ns * 3, "noise");
-  rc = rc ? rc : dalloc(c, &c->bead_id, ns, "bead ids");
-  rc = rc ? rc : dalloc(c, &c->slot_of, ns, "slots");
-  rc = rc ? rc : dalloc(c, &c->bond_nbr, ns * 3, "bonds");
-  rc = rc ? rc : dalloc(c, &c->bond_info, ns, "bonds");
-  rc = rc ? rc : dalloc(c, &c->types_dev, ns, "types");
-  rc = rc ? rc : dalloc(c, &c->bondk_dev, TILD_MAX_BOND_TYPES, "bond constants");
-  rc = rc ? rc : dalloc(c, &c->bondr_dev, TILD_MAX_BOND_TYPES, "bond constants");
-  if (c->C) rc = rc ? rc : dalloc(c, &c->charge, ns, "charges");
-  rc = rc ? rc : dalloc(c, &c->rho, nch * M, "densities");
-  rc = rc ? rc : dalloc(c, &c->rho_fx, nch * M, "density accumulator");
-  rc = rc ? rc : dalloc(c, &c->rhok, nch * Mh, "density spectra");
-  rc = rc ? rc : dalloc(c, &c->gk, nch * c->D * Mh, "force spectra");
-  rc = rc ? rc : dalloc(c, &c->gfield, nch * c->D * M, "force fields");
-  rc = rc ? rc : dalloc(c, &c->g4, nch * M, "interleaved force fields");
-  rc = rc ? rc : dalloc(c, &c->utab, nfft * Mh, "multiplier tables");
-  rc = rc ? rc : dalloc(c, &c->virk, nfft * c->nP * Mh, "virial tables");
-  if (c->C) rc = rc ? rc : dalloc(c, &c->ctab, Mh, "charge table");
-  if (!c->fields.empty()) rc = rc ? rc : dalloc(c, &c->frfield, c->fields.size() * c->D * M, "fieldphase fields");
-  rc = rc ? rc : dalloc(c, &c->kd, (size_t)g.nx[0] + g.nx[1] + g.nx[2], "k vectors");
-  rc = rc ? rc : dalloc(c, &c->kk, (size_t)g.nx[0] + g.nx[1] + g.nx[2], "k vectors");
-  rc = rc ? rc : dalloc(c, &c->xfer, ns * 3, "transfer buffer");
-  rc = rc ? rc : dalloc(c, &c->d_status, 1, "status");
-  if (cfg->rng == TILD_RNG_XORWOW) rc = rc ? rc : dalloc(c, &c->xorwow, ns, "xorwow states");
-  if (rc) {
-    fprintf(stderr, "tild_create: %s\n", c->err.c_str());
-    free_all(c);
-    delete c;
-    return rc;
-  }
-  cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream);
-  cudaMemsetAsync(c->rho_fx, 0, sizeof(unsigned long long) * nch * M, c->stream);
-  cudaMemsetAsync(c->noise, 0, sizeof(float) * ns * 3, c->stream);
-  {
-    std::vector<float> bk(TILD_MAX_BOND_TYPES, 0.f), br(TILD_MAX_BOND_TYPES, 0.f);
-    for (int b = 0; b < cfg->n_bond_types; b++) {
-      bk[b] = cfg->bond_k[b];
-      br[b] = cfg->bond_req[b];
-    }
-    cudaMemcpyAsync(c->bondk_dev, bk.data(), bk.size() * 4, cudaMemcpyHostToDevice, c->stream);
-    cudaMemcpyAsync(c->bondr_dev, br.data(), br.size() * 4, cudaMemcpyHostToDevice, c->stream);
-    // identity slot order until the first sort
-    std::vector<int> id(ns);
-    for (size_t i = 0; i < ns; i++) id[i] = (int)i;
-    cudaMemcpyAsync(c->bead_id, id.data(), ns * 4, cudaMemcpyHostToDevice, c->stream);
-    cudaMemcpyAsync(c->slot_of, id.data(), ns * 4, cudaMemcpyHostToDevice, c->stream);
-    if (tild_check(c, cudaStreamSynchronize(c->stream), "upload constants")) rc = TILD_ERR_CUDA;
-  }
-  // cuFFT plans: batched R2C over all density channels, batched C2R over channel x direction
-  if (!rc) {
-    int n[3];
-    if (c->D == 3) { n[0] = g.nx[2]; n[1] = g.nx[1]; n[2] = g.nx[0]; }
-    else { n[0] = g.nx[1]; n[1] = g.nx[0]; }
-    if (tild_check_fft(c, cufftPlanMany(&c->plan_r2c, c->D, n, nullptr, 1, (int)M, nullptr, 1, (int)Mh, CUFFT_R2C, (int)nch), "plan R2C") ||
-        tild_check_fft(c, cufftPlanMany(&c->plan_c2r, c->D, n, nullptr, 1, (int)Mh, nullptr, 1, (int)M, CUFFT_C2R, (int)(nch * c->D)), "plan C2R") ||
-        tild_check_fft(c, cufftSetStream(c->plan_r2c, c->stream), "plan stream") ||
-        tild_check_fft(c, cufftSetStream(c->plan_c2r, c->stream), "plan stream"))
-      rc = TILD_ERR_CUDA;
-    else
-      c->plans = true;
-  }
-  c->sort_interval = cfg->sort_interval == 0 ? 16 : (cfg->sort_interval < 0 ? 0 : cfg->sort_interval);
-  if (!rc && c->sort_interval > 0) rc = tild_sort_alloc(c);
-  if (!rc) rc = tild_build_tables(c);
+  tild_batch* c = new tild_batch();
+  const int rc = engine_create(cfgs, nsys, device, c);
   if (rc) {
     fprintf(stderr, "tild_create: %s\n", c->err.c_str());
     free_all(c);
@@ -352,211 +704,65 @@ int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
   return TILD_OK;
 }
 
+int32_t tild_create(const tild_config* cfg, int32_t device, tild_ctx** out) {
+  if (!cfg || !out) return TILD_ERR_BAD_INPUT;
+  tild_batch* b = nullptr;
+  const int rc = create_common(cfg, 1, device, &b);
+  *out = b;
+  return rc;
+}
+
 int32_t tild_destroy(tild_ctx* c) {
   if (!c) return TILD_ERR_BAD_INPUT;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
-  delete c;
+  delete static_cast<tild_batch*>(c);
   return TILD_OK;
 }
 
 int32_t tild_set_topology(tild_ctx* c, const int32_t* types, const float* charges, const int32_t* n_bonds,
                           const int32_t* bonded_to, const int32_t* bond_type) {
-  if (!c || !types) return TILD_ERR_BAD_INPUT;
-  if (c->C && !charges) return set_err(c, TILD_ERR_BAD_INPUT, "charges required when do_charges is set");
-  cudaSetDevice(c->device);
-  const int ns = c->ns;
-  std::vector<int> slot_of(ns), bead_id(ns);
-  if (tild_check(c, cudaMemcpyAsync(slot_of.data(), c->slot_of, ns * 4, cudaMemcpyDeviceToHost, c->stream), "slots") ||
-      tild_check(c, cudaMemcpyAsync(bead_id.data(), c->bead_id, ns * 4, cudaMemcpyDeviceToHost, c->stream), "ids") ||
-      tild_check(c, cudaStreamSynchronize(c->stream), "sync"))
-    return TILD_ERR_CUDA;
-  std::vector<int> nbr(3 * (size_t)ns, 0), info(ns, 0);
-  std::vector<float> q;
-  if (c->C) q.resize(ns);
-  for (int b = 0; b < ns; b++) {
-    if (types[b] < 0 || types[b] >= c->T) return set_err(c, TILD_ERR_BAD_INPUT, "bead type out of range");
-    const int s = slot_of[b];
-    int nb = n_bonds ? n_bonds[b] : 0;
-    if (nb < 0 || nb > TILD_MAX_BONDS) return set_err(c, TILD_ERR_BAD_INPUT, "more than MAX_BONDS (3) bonds on a bead");
-    int in = nb;
-    for (int k = 0; k < nb; k++) {
-      const int j = bonded_to[3 * (size_t)b + k], bt = bond_type[3 * (size_t)b + k];
-      if (j < 0 || j >= ns) return set_err(c, TILD_ERR_BAD_INPUT, "bond partner out of range");
-      if (bt < 0 || bt >= c->cfg.n_bond_types) return set_err(c, TILD_ERR_BAD_INPUT, "bond type out of range");
-      nbr[3 * (size_t)s + k] = slot_of[j];
-      in |= bt << (8 + 8 * k);
-    }
-    info[s] = in;
-    if (c->C) q[s] = charges[b];
-  }
-  if (tild_check(c, cudaMemcpyAsync(c->bond_nbr, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, c->stream), "bonds") ||
-      tild_check(c, cudaMemcpyAsync(c->bond_info, info.data(), info.size() * 4, cudaMemcpyHostToDevice, c->stream), "bonds") ||
-      tild_check(c, cudaMemcpyAsync(c->types_dev, types, (size_t)ns * 4, cudaMemcpyHostToDevice, c->stream), "types") ||
-      (c->C && tild_check(c, cudaMemcpyAsync(c->charge, q.data(), (size_t)ns * 4, cudaMemcpyHostToDevice, c->stream), "charges")) ||
-      tild_check(c, cudaStreamSynchronize(c->stream), "sync topology"))
-    return TILD_ERR_CUDA;
-  // fixed-point scale of the shared-memory spread: 256 beads x the largest product of stencil
-  // weights (times the largest |q| on the charge channel) must stay below 2^31
-  {
-    double wmax = 0.0;
-    for (int k = 0; k <= 1000; k++) {
-      const double sx = -0.5 + k / 1000.0;
-      double W[5];
-      const int P = c->p;
-      double sx2 = sx * sx, sx3, sx4;
-      if (P == 0) { W[0] = 1; }
-      else if (P == 1) { W[0] = 0.5 - sx; W[1] = 0.5 + sx; }
-      else if (P == 2) { W[0] = 0.125 - 0.5 * sx + 0.5 * sx2; W[1] = 0.75 - sx2; W[2] = 0.125 + 0.5 * sx + 0.5 * sx2; }
-      else if (P == 3) { sx3 = sx2 * sx; W[0] = (1 - 6 * sx + 12 * sx2 - 8 * sx3) / 48; W[1] = (23 - 30 * sx - 12 * sx2 + 24 * sx3) / 48;
-                         W[2] = (23 + 30 * sx - 12 * sx2 - 24 * sx3) / 48; W[3] = (1 + 6 * sx + 12 * sx2 + 8 * sx3) / 48; }
-      else { sx3 = sx2 * sx2; sx4 = sx2 * sx2; W[0] = (1 - 8 * sx + 24 * sx2 - 32 * sx3 + 16 * sx4) / 384;
-             W[1] = (19 - 44 * sx + 24 * sx2 + 16 * sx3 - 16 * sx4) / 96; W[2] = (115 - 120 * sx2 + 48 * sx4) / 192;
-             W[3] = (19 + 44 * sx + 24 * sx2 - 16 * sx3 - 16 * sx4) / 96; W[4] = (1 + 8 * sx + 24 * sx2 + 32 * sx3 + 16 * sx4) / 384; }
-      for (int a = 0; a <= P; a++) wmax = std::max(wmax, std::fabs(W[a]));
-    }
-    double qmax = 1.0;
-    if (c->C)
-      for (int b = 0; b < ns; b++) qmax = std::max(qmax, (double)std::fabs(charges[b]));
-    const double bound = 256.0 * std::pow(wmax * 1.05, c->D) / (double)c->g.gvol * qmax;
-    int k = 0;
-    while (k < 31 && bound * std::ldexp(1.0, k + 1) < 2147483647.0) k++;
-    c->spread_kbits = k;
-  }
-  c->topo_set = true;
-  return TILD_OK;
+  return sys_set_topology(c, 0, types, charges, n_bonds, bonded_to, bond_type);
 }
 
 int32_t tild_set_state(tild_ctx* c, const float* x, const float* xo, const float* prev_noise) {
-  if (!c || !x) return TILD_ERR_BAD_INPUT;
-  if (!c->topo_set) return set_err(c, TILD_ERR_STATE, "tild_set_topology must come before tild_set_state");
-  cudaSetDevice(c->device);
-  const size_t n = (size_t)c->ns * c->D;
-  for (size_t i = 0; i < n; i++)
-    if (!std::isfinite(x[i])) return set_err(c, TILD_ERR_NAN, "non-finite position in tild_set_state");
-  const unsigned nb = nblk(c->ns, 256);
-  if (tild_check(c, cudaMemcpyAsync(c->xfer, x, n * 4, cudaMemcpyHostToDevice, c->stream), "upload x")) return TILD_ERR_CUDA;
-  k_pack_pos<<<nb, 256, 0, c->stream>>>(c->xfer, c->types_dev, c->slot_of, c->ns, c->D, c->pos[c->cur]);
-  c->launches++;
-  // x_{n-1}: xo when given, else x (send_3n_to_device copies x into xo, device_comm_utils.cu:15-16)
-  if (xo && tild_check(c, cudaMemcpyAsync(c->xfer, xo, n * 4, cudaMemcpyHostToDevice, c->stream), "upload xo"))
-    return TILD_ERR_CUDA;
-  k_pack_pos<<<nb, 256, 0, c->stream>>>(c->xfer, c->types_dev, c->slot_of, c->ns, c->D, c->pos[c->cur ^ 1]);
-  c->launches++;
-  if (prev_noise && tild_check(c, cudaMemcpyAsync(c->xfer, prev_noise, n * 4, cudaMemcpyHostToDevice, c->stream), "upload noise"))
-    return TILD_ERR_CUDA;
-  k_pack_noise<<<nb, 256, 0, c->stream>>>(prev_noise ? c->xfer : nullptr, c->slot_of, c->ns, c->D, c->noise);
-  c->launches++;
-  if (c->cfg.rng == TILD_RNG_XORWOW) {
-    k_init_xorwow<<<nb, 256, 0, c->stream>>>(c->xorwow, c->bead_id, c->ns, (unsigned int)c->cfg.seed);
-    c->launches++;
-  }
-  if (c->sort_interval > 0) {
-    int rs = tild_sort_beads(c);
-    if (rs) return rs;
-  }
-  if (tild_check(c, cudaStreamSynchronize(c->stream), "set state")) return TILD_ERR_CUDA;
-  c->state_set = true;
-  c->have_forces = false;
-  return TILD_OK;
+  return sys_set_state(c, 0, x, xo, prev_noise);
 }
 
-int32_t tild_get_state(tild_ctx* c, float* x, float* xo, float* prev_noise) {
-  if (!c) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
-  cudaSetDevice(c->device);
-  const size_t n = (size_t)c->ns * c->D;
-  const unsigned nb = nblk(c->ns, 256);
-  float* outs[3] = {x, xo, prev_noise};
-  for (int k = 0; k < 3; k++) {
-    if (!outs[k]) continue;
-    if (k < 2) k_unpack_pos<<<nb, 256, 0, c->stream>>>(c->pos[k == 0 ? c->cur : c->cur ^ 1], c->bead_id, c->ns, c->D, c->xfer);
-    else k_unpack_noise<<<nb, 256, 0, c->stream>>>(c->noise, c->bead_id, c->ns, c->D, c->xfer);
-    c->launches++;
-    if (tild_check(c, cudaMemcpyAsync(outs[k], c->xfer, n * 4, cudaMemcpyDeviceToHost, c->stream), "download") ||
-        tild_check(c, cudaStreamSynchronize(c->stream), "sync download"))
-      return TILD_ERR_CUDA;
-  }
-  return TILD_OK;
-}
+int32_t tild_get_state(tild_ctx* c, float* x, float* xo, float* prev_noise) { return sys_get_state(c, 0, x, xo, prev_noise); }
 
-int32_t tild_forces(tild_ctx* c, float* f) {
-  if (!c) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "tild_set_state must come before tild_forces");
-  cudaSetDevice(c->device);
-  int rc = tild_run_forces(c, c->step, false, f ? c->xfer : nullptr);
-  if (rc) return rc;
-  rc = tild_poll_status(c);
-  if (rc) return rc;
-  if (f) {
-    if (tild_check(c, cudaMemcpyAsync(f, c->xfer, (size_t)c->ns * c->D * 4, cudaMemcpyDeviceToHost, c->stream), "download f") ||
-        tild_check(c, cudaStreamSynchronize(c->stream), "sync f"))
-      return TILD_ERR_CUDA;
-  }
-  return TILD_OK;
-}
+int32_t tild_forces(tild_ctx* c, float* f) { return sys_forces(c, 0, f); }
 
 int32_t tild_step(tild_ctx* c, int32_t nsteps) {
   if (!c || nsteps < 0) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "tild_set_state must come before tild_step");
-  cudaSetDevice(c->device);
-  for (int k = 0; k < nsteps; k++) {
-    const int64_t s = c->step + 1;
-    int rc = tild_run_forces(c, s, true, nullptr);
-    if (rc) return rc;
-    c->step = s;
-  }
-  return tild_poll_status(c);
+  return engine_step(c, nsteps);
 }
 
 int32_t tild_get_step(tild_ctx* c, int64_t* step) {
   if (!c || !step) return TILD_ERR_BAD_INPUT;
-  *step = c->step;
+  *step = c->sys[0].step;
   return TILD_OK;
 }
 
-int32_t tild_set_step(tild_ctx* c, int64_t step) {
-  if (!c || step < 0) return TILD_ERR_BAD_INPUT;
-  c->step = step;
-  return TILD_OK;
-}
+int32_t tild_set_step(tild_ctx* c, int64_t step) { return sys_set_step(c, 0, step); }
 
-int32_t tild_observables(tild_ctx* c, tild_obs* o) {
-  if (!c || !o) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
-  cudaSetDevice(c->device);
-  if (!c->have_forces) {
-    int rc = tild_run_forces(c, c->step, false, nullptr);
-    if (rc) return rc;
-  }
-  int rc = tild_obs_compute(c, o);
-  if (rc) return rc;
-  if (!std::isfinite(o->upe)) return set_err(c, TILD_ERR_NAN, "non-finite energy");
-  return tild_poll_status(c);
-}
+int32_t tild_observables(tild_ctx* c, tild_obs* o) { return sys_observables(c, 0, o); }
 
-int32_t tild_get_density(tild_ctx* c, float* rho) {
-  if (!c || !rho) return TILD_ERR_BAD_INPUT;
-  if (!c->have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
-  cudaSetDevice(c->device);
-  if (tild_check(c, cudaMemcpyAsync(rho, c->rho, sizeof(float) * (size_t)(c->T + c->C) * c->g.M, cudaMemcpyDeviceToHost, c->stream), "download rho") ||
-      tild_check(c, cudaStreamSynchronize(c->stream), "sync rho"))
-    return TILD_ERR_CUDA;
-  return TILD_OK;
-}
+int32_t tild_get_density(tild_ctx* c, float* rho) { return sys_density(c, 0, rho); }
 
 int32_t tild_get_stencil(tild_ctx* c, int32_t* inds, float* w) {
   if (!c) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  const SysHost& h = c->sys[0];
+  if (!h.state_set) return set_err(c, TILD_ERR_STATE, "no state");
   cudaSetDevice(c->device);
-  const size_t n = (size_t)c->ns * c->S;
+  const size_t n = (size_t)h.ns * h.S;
   int* di = nullptr;
   float* dw = nullptr;
   int rc = TILD_OK;
   if (inds && dalloc(c, &di, n, "stencil indices")) rc = TILD_ERR_OOM;
   if (!rc && w && dalloc(c, &dw, n, "stencil weights")) rc = TILD_ERR_OOM;
-  if (!rc) rc = tild_stencil_run(c, di, dw);
+  if (!rc) rc = tild_stencil_run(c, 0, di, dw);
   if (!rc && inds && tild_check(c, cudaMemcpyAsync(inds, di, n * 4, cudaMemcpyDeviceToHost, c->stream), "download")) rc = TILD_ERR_CUDA;
   if (!rc && w && tild_check(c, cudaMemcpyAsync(w, dw, n * 4, cudaMemcpyDeviceToHost, c->stream), "download")) rc = TILD_ERR_CUDA;
   if (!rc && tild_check(c, cudaStreamSynchronize(c->stream), "sync")) rc = TILD_ERR_CUDA;
@@ -566,25 +772,26 @@ int32_t tild_get_stencil(tild_ctx* c, int32_t* inds, float* w) {
 }
 
 int32_t tild_sk_accumulate(tild_ctx* c, int32_t slot, int32_t type) {
-  if (!c || slot < 0 || slot >= TILD_MAX_COMPUTES || type < 0 || type >= c->T) return TILD_ERR_BAD_INPUT;
-  if (!c->have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
+  if (!c || slot < 0 || slot >= TILD_MAX_COMPUTES || type < 0 || type >= c->sys[0].T) return TILD_ERR_BAD_INPUT;
+  if (!c->sys[0].have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
   cudaSetDevice(c->device);
-  return tild_sk_acc_run(c, slot, type);
+  return tild_sk_acc_run(c, 0, slot, type);
 }
 
 int32_t tild_sk_get(tild_ctx* c, int32_t slot, double* sk, int32_t* ncalls) {
   if (!c || slot < 0 || slot >= TILD_MAX_COMPUTES) return TILD_ERR_BAD_INPUT;
   cudaSetDevice(c->device);
-  const int n = c->sk[slot] ? c->sk_calls[slot] : 0;
+  const SysHost& h = c->sys[0];
+  const int n = h.sk[slot] ? h.sk_calls[slot] : 0;
   if (ncalls) *ncalls = n;
   if (!sk) return TILD_OK;
-  const Geom& g = c->g;
+  const Geom& g = h.g;
   if (n == 0) {
     memset(sk, 0, sizeof(double) * 2 * (size_t)g.M);
     return TILD_OK;
   }
-  std::vector<double> h(2 * (size_t)g.Mh);
-  if (tild_check(c, cudaMemcpyAsync(h.data(), c->sk[slot], sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream), "download sk") ||
+  std::vector<double> hb(2 * (size_t)g.Mh);
+  if (tild_check(c, cudaMemcpyAsync(hb.data(), h.sk[slot], sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, c->stream), "download sk") ||
       tild_check(c, cudaStreamSynchronize(c->stream), "sync sk"))
     return TILD_ERR_CUDA;
   // expand the half spectrum: A(-k) = conj(A(k)) for A = rho_k * rho_k of a real density
@@ -596,13 +803,13 @@ int32_t tild_sk_get(tild_ctx* c, int32_t slot, double* sk, int32_t* ncalls) {
         double re, im;
         if (x < g.nxh) {
           const size_t h2 = (size_t)x + (size_t)g.nxh * (y + (size_t)N1 * z);
-          re = h[2 * h2];
-          im = h[2 * h2 + 1];
+          re = hb[2 * h2];
+          im = hb[2 * h2 + 1];
         } else {
           const int xm = N0 - x, ym = (N1 - y) % N1, zm = (N2 - z) % N2;
           const size_t h2 = (size_t)xm + (size_t)g.nxh * (ym + (size_t)N1 * zm);
-          re = h[2 * h2];
-          im = -h[2 * h2 + 1];
+          re = hb[2 * h2];
+          im = -hb[2 * h2 + 1];
         }
         sk[2 * id] = re / n;
         sk[2 * id + 1] = im / n;
@@ -612,20 +819,21 @@ int32_t tild_sk_get(tild_ctx* c, int32_t slot, double* sk, int32_t* ncalls) {
 
 int32_t tild_nlist_build(tild_ctx* c, float rc, int32_t group_type, int32_t* cell_of, int32_t* neigh_count,
                          int32_t* neigh, int32_t* cell_max_out) {
-  if (!c || !(rc > 0.f) || group_type < -1 || group_type >= c->T) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  if (!c || !(rc > 0.f) || group_type < -1 || group_type >= c->sys[0].T) return TILD_ERR_BAD_INPUT;
+  const SysHost& h = c->sys[0];
+  if (!h.state_set) return set_err(c, TILD_ERR_STATE, "no state");
   cudaSetDevice(c->device);
   int nc[3], total, cmax;
   float Lc[3];
-  if (tild_nlist_geom(c, rc, nc, Lc, &total, &cmax)) return set_err(c, TILD_ERR_BAD_INPUT, "cutoff larger than the box");
+  if (tild_nlist_geom(h, rc, nc, Lc, &total, &cmax)) return set_err(c, TILD_ERR_BAD_INPUT, "cutoff larger than the box");
   if (cell_max_out) *cell_max_out = cmax;
   if (!cell_of && !neigh_count && !neigh) return TILD_OK;
-  const size_t ns = c->ns;
+  const size_t ns = h.ns;
   int *dc = nullptr, *dn = nullptr, *dl = nullptr;
   int r = TILD_OK;
   if (dalloc(c, &dc, ns, "nlist") || dalloc(c, &dn, ns, "nlist") || dalloc(c, &dl, ns * (size_t)std::max(cmax, 1), "nlist"))
     r = TILD_ERR_OOM;
-  if (!r) r = tild_nlist_run(c, rc, group_type, dc, dn, dl);
+  if (!r) r = tild_nlist_run(c, 0, rc, group_type, dc, dn, dl);
   int st = r ? r : tild_poll_status(c);
   if (!r) {
     if ((cell_of && tild_check(c, cudaMemcpy(cell_of, dc, ns * 4, cudaMemcpyDeviceToHost), "download")) ||
@@ -639,44 +847,18 @@ int32_t tild_nlist_build(tild_ctx* c, float rc, int32_t group_type, int32_t* cel
   return r ? r : st;
 }
 
-int32_t tild_time_steps(tild_ctx* c, int32_t nsteps, double* ms) {
-  if (!c || !ms || nsteps < 0) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
-  cudaSetDevice(c->device);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, c->stream);
-  int rc = TILD_OK;
-  for (int k = 0; k < nsteps && !rc; k++) {
-    const int64_t s = c->step + 1;
-    rc = tild_run_forces(c, s, true, nullptr);
-    if (!rc) c->step = s;
-  }
-  cudaEventRecord(e1, c->stream);
-  cudaEventSynchronize(e1);
-  float t = 0.f;
-  cudaEventElapsedTime(&t, e0, e1);
-  *ms = t;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  return rc ? rc : tild_poll_status(c);
-}
+int32_t tild_time_steps(tild_ctx* c, int32_t nsteps, double* ms) { return engine_time(c, nsteps, ms); }
 
 int32_t tild_profile_steps(tild_ctx* c, int32_t nsteps, double* stage_ms, int32_t max_stages, int32_t* n_stages,
                            char* names, int32_t name_cap) {
   if (!c || !stage_ms || nsteps < 0) return TILD_ERR_BAD_INPUT;
-  if (!c->state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "no state");
   cudaSetDevice(c->device);
   c->prof_ev.clear();
   c->prof_stage.clear();
   c->profiling = true;
   int rc = TILD_OK;
-  for (int k = 0; k < nsteps && !rc; k++) {
-    const int64_t s = c->step + 1;
-    rc = tild_run_forces(c, s, true, nullptr);
-    if (!rc) c->step = s;
-  }
+  for (int k = 0; k < nsteps && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
   c->profiling = false;
   cudaEvent_t last;
   cudaEventCreate(&last);
@@ -718,5 +900,42 @@ int32_t tild_sync(tild_ctx* c) {
   cudaSetDevice(c->device);
   return tild_poll_status(c);
 }
+
+// ---- batches ------------------------------------------------------------------------------
+int32_t tild_batch_create(const tild_config* cfgs, int32_t nsys, int32_t device, tild_batch** out) {
+  return create_common(cfgs, nsys, device, out);
+}
+int32_t tild_batch_destroy(tild_batch* b) { return tild_destroy(b); }
+const char* tild_batch_last_error(const tild_batch* b) { return tild_last_error(b); }
+int32_t tild_batch_set_topology(tild_batch* b, int32_t sys, const int32_t* types, const float* charges,
+                                const int32_t* n_bonds, const int32_t* bonded_to, const int32_t* bond_type) {
+  return sys_set_topology(b, sys, types, charges, n_bonds, bonded_to, bond_type);
+}
+int32_t tild_batch_set_state(tild_batch* b, int32_t sys, const float* x, const float* xo, const float* prev_noise) {
+  return sys_set_state(b, sys, x, xo, prev_noise);
+}
+int32_t tild_batch_get_state(tild_batch* b, int32_t sys, float* x, float* xo, float* prev_noise) {
+  return sys_get_state(b, sys, x, xo, prev_noise);
+}
+int32_t tild_batch_set_active(tild_batch* b, int32_t sys, int32_t active) {
+  if (check_sys(b, sys)) return TILD_ERR_BAD_INPUT;
+  b->sys[sys].active = active != 0;
+  return tild_upload_sys(b);
+}
+int32_t tild_batch_set_step(tild_batch* b, int32_t sys, int64_t step) { return sys_set_step(b, sys, step); }
+int32_t tild_batch_get_step(tild_batch* b, int32_t sys, int64_t* step) {
+  if (check_sys(b, sys) || !step) return TILD_ERR_BAD_INPUT;
+  *step = b->sys[sys].step;
+  return TILD_OK;
+}
+int32_t tild_batch_step(tild_batch* b, int32_t nsteps) {
+  if (!b || nsteps < 0) return TILD_ERR_BAD_INPUT;
+  return engine_step(b, nsteps);
+}
+int32_t tild_batch_forces(tild_batch* b, int32_t sys, float* f) { return sys_forces(b, sys, f); }
+int32_t tild_batch_observables(tild_batch* b, int32_t sys, tild_obs* o) { return sys_observables(b, sys, o); }
+int32_t tild_batch_get_density(tild_batch* b, int32_t sys, float* rho) { return sys_density(b, sys, rho); }
+int32_t tild_batch_time_steps(tild_batch* b, int32_t nsteps, double* ms) { return engine_time(b, nsteps, ms); }
+int32_t tild_batch_sync(tild_batch* b) { return tild_sync(b); }
 
 }  // extern "C"

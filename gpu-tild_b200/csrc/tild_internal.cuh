@@ -1,19 +1,25 @@
-// tild_internal.cuh — device state of one TILD system and the device helpers shared by the
-// kernels of libtild.
+// tild_internal.cuh — device state of a TILD engine (one or many independent systems on one
+// GPU) and the device helpers shared by the kernels of libtild.
 //
-// HBM layout of a context (ns beads, M = prod(Nx) grid points, Mh = M/Nx*(Nx/2+1) half-spectrum
-// points, T types, C = 1 with charges, D = dim):
-//   pos[2]     float4[ns]   (x, y, z, type bits in .w); pos[cur] = x_n, pos[cur^1] = x_{n-1}
-//   noise      float[ns*3]  GJF previous noise (reference d_prev_noise)
-//   bead_id    int[ns]      original bead index of each slot (slots are re-ordered by the sort)
-//   bond_nbr   int[ns*3]    partner slots; bond_info int[ns] = n | t0<<8 | t1<<16 | t2<<24
-//   rho        float[(T+C)*M]        densities (spread), x fastest like the reference
-//   rhok       cufftComplex[(T+C)*Mh] R2C of rho
-//   gk         cufftComplex[(T+C)*D*Mh] -i k_d Phi_t(k): input of the batched C2R
-//   gfield     float[(T+C)*D*M]      -grad of the convolved potential per type (and E field)
-//   g4         float4[(T+C)*M]       the same, interleaved per grid point for the gather
-//   utab       float[nfft_styles*Mh]  u_s(k)/M per FFT pair style
-//   virk       cufftComplex[nfft_styles*nP*Mh] virial kernels / M^2
+// An engine holds S systems that share dim and pmeorder.  Every per-step kernel covers all
+// systems in one launch: particle kernels map a CTA (256 slots) to one system through a lookup
+// table, grid kernels map a CTA of grid points the same way, and the FFTs run as one batched
+// cuFFT plan per grid shape ("bucket").  A single-system context is an engine with S = 1.
+//
+// HBM layout (all arrays concatenated over systems; per-system offsets live in SysDev):
+//   pos[2]     float4[NSP]  (x, y, z, type bits in .w); pos[cur] = x_n, pos[cur^1] = x_{n-1}
+//              NSP = sum over systems of ns rounded up to 256; padding slots carry type 0xff
+//   noise      float[3*NSP] GJF previous noise (reference d_prev_noise)
+//   bead_id    int[NSP]     bead index within its system (-1 for padding)
+//   bond_nbr   int[3*NSP]   partner slots (absolute); bond_info int[NSP] = n | t0<<8 | t1<<16 | t2<<24
+//   rho_fx     u64[CH*M]    fixed-point density accumulators, CH channels = T + C per system
+//   rho        f32[CH*M]    densities (x fastest like the reference)
+//   rhok       c64[CH*Mh]   R2C of rho
+//   gk         c64[CH*D*Mh] -i k_d Phi_t(k): input of the batched C2R
+//   gfield     f32[CH*D*M]  -grad of the convolved potential (and E field), planar
+//   g4         float4[CH*M] the same interleaved per grid point for the gather
+//   utab       f32[sum nfft*Mh]          u_s(k)/M per FFT pair style
+//   virk       c64[sum nfft*nP*Mh]       virial kernels / M^2
 #pragma once
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -23,7 +29,7 @@
 #include <vector>
 #include "../../include/tild.h"
 
-#define TILD_MAXT_FAST 4   // kernels are specialised for up to this many channels
+#define TILD_MAXT_FAST 4   // k-space kernels are specialised for up to this many channels
 
 // Device status word bits (reference: die() / NaN checks; here a flag the host polls).
 enum : int {
@@ -31,6 +37,9 @@ enum : int {
   ST_INDEX_RANGE = 2,
   ST_NLIST_OVERFLOW = 4,
 };
+
+constexpr int kTile = 256;            // slots per particle CTA (systems are padded to it)
+constexpr int kPadType = 0xff;        // type bits of a padding slot
 
 struct Geom {
   int nx[3];
@@ -42,79 +51,123 @@ struct Geom {
   long long M, Mh;
 };
 
-struct StyleK {     // one FFT pair style as the k-space kernels see it
-  int a, b;         // types
-  int ramp;
-  float Ai, Af;     // prefactors for the ramp
-  float uk0;        // u_k(0) of the unscaled table (ramp denominator)
+// Per-system descriptor read by the kernels (one per system, in device memory).
+struct SysDev {
+  Geom g;
+  int T, C, kbits, nfft;
+  int slot0, ns, ns_pad, bead0;
+  int active;                      // 0: skipped by the particle kernels
+  long long grid0;                 // channel 0 of this system in rho / rho_fx / g4 (grid points)
+  long long spec0;                 // channel 0 in rhok (half-spectrum points)
+  long long utab0, ctab0, kd0;     // offsets in utab, ctab, kd
+  long long step;                  // completed steps (advanced on the device)
+  int max_steps;
+  int sa[TILD_MAX_STYLES], sb[TILD_MAX_STYLES], sramp[TILD_MAX_STYLES];
+  float sAi[TILD_MAX_STYLES], sAf[TILD_MAX_STYLES], suk0[TILD_MAX_STYLES];
+  uint64_t seed;
+  float delt, noise_mag;
+  int n_integ;
+  int integ_kind[TILD_MAX_INTEGRATORS];
+  int type_mask[TILD_MAX_TYPES];
+  float mass[TILD_MAX_TYPES], diff[TILD_MAX_TYPES];
+  float bond_k[TILD_MAX_BOND_TYPES], bond_req[TILD_MAX_BOND_TYPES];
 };
 
 struct FieldK {     // one fieldphase style
-  int a, b;
-  int slot;         // index into frfield
+  int sys, a, b;
+  int cfg_index;
+  long long fr0;    // offset of its static field in frfield
 };
 
-struct tild_ctx {
+// Host-side bookkeeping of one system.
+struct SysHost {
   tild_config cfg;
-  int device = 0;
-  cudaStream_t stream = nullptr;
   int D = 3, T = 1, C = 0, ns = 0, p = 1, S = 1, nP = 6;
   Geom g;
   double dV = 1.0, V = 1.0;
-  int max_steps = 0;
-
-  // style bookkeeping
-  std::vector<int> fft_style_index;   // config style index -> fft table slot (-1 if fieldphase)
-  std::vector<StyleK> styles_k;       // per fft table slot
-  std::vector<int> fft_style_cfg;     // fft table slot -> config style index
-  std::vector<FieldK> fields;
+  int slot0 = 0, ns_pad = 0, bead0 = 0;  // bead0: first bead in the engine's bead numbering
+  long long grid0 = 0, spec0 = 0, utab0 = 0, ctab0 = 0, kd0 = 0, virk0 = 0;
+  int kbits = 20;
+  std::vector<int> fft_cfg;              // fft table slot -> config style index
   int type_integ_mask[TILD_MAX_TYPES] = {0};
+  int bucket = 0;
+  int64_t step = 0, forces_step = 0;
+  bool topo_set = false, state_set = false, have_forces = false, active = true;
+  double* sk[TILD_MAX_COMPUTES] = {nullptr};
+  int sk_calls[TILD_MAX_COMPUTES] = {0};
+};
+
+struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R plan
+  int nx[3];
+  std::vector<int> systems;
+  long long grid0 = 0, spec0 = 0;        // first channel of the bucket
+  int channels = 0;
+  cufftHandle r2c = 0, c2r = 0;
+  bool planned = false;
+};
+
+struct tild_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int D = 3, P = 1;
+  int nsys = 1;
+  std::vector<SysHost> sys;
+  std::vector<Bucket> buckets;
+  std::vector<FieldK> fields;
+  SysDev* d_sys = nullptr;
+  std::vector<SysDev> h_sys;             // host mirror of d_sys
+  int rng = TILD_RNG_PHILOX;
+  int maxT = 1;                          // largest channel count of a system (T + C)
+  bool any_charges = false;
+
+  // lookup tables: CTA -> system
+  int* cta_bead = nullptr;  int n_cta_bead = 0;    // 256-slot blocks
+  int* cta_spec = nullptr;  int n_cta_spec = 0;    // 256-point blocks of half spectra
+  int* cta_grid = nullptr;  int n_cta_grid = 0;    // 256-point blocks of real grids
+  std::vector<long long> spec_block0, grid_block0; // first block of each system
 
   // bead state
+  int nslots = 0;
   float4* pos[2] = {nullptr, nullptr};
   int cur = 0;
   float* noise = nullptr;
   int* bead_id = nullptr;
-  int* slot_of = nullptr;
+  int* slot_of = nullptr;                // engine bead index -> slot
   int* bond_nbr = nullptr;
   int* bond_info = nullptr;
   float* charge = nullptr;
-  float* bondk_dev = nullptr;         // bond constants [TILD_MAX_BOND_TYPES]
-  float* bondr_dev = nullptr;
-  int* types_dev = nullptr;           // per bead (bead order), kept for re-packing
+  int* types_dev = nullptr;
   curandStateXORWOW_t* xorwow = nullptr;
+  int nbeads = 0;
 
   // grids
-  unsigned long long* rho_fx = nullptr;  // fixed-point (2^32) density accumulator [(T+C)*M]
+  long long grid_total = 0, spec_total = 0;  // channels x points
+  unsigned long long* rho_fx = nullptr;
   float* rho = nullptr;
   cufftComplex* rhok = nullptr;
   cufftComplex* gk = nullptr;
   float* gfield = nullptr;
-  float4* g4 = nullptr;                  // interleaved force field [(T+C)][M] (gather input)
+  float4* g4 = nullptr;
   float* utab = nullptr;
-  float* ctab = nullptr;              // charge force multiplier [Mh]
+  float* ctab = nullptr;
   cufftComplex* virk = nullptr;
-  float* frfield = nullptr;           // [nfields*D*M]
-  float* kd = nullptr;                // derivative k per axis: [nx0 + nx1 + nx2], Nyquist = 0
-  float* kk = nullptr;                // k per axis for k^2: [nx0 + nx1 + nx2]
+  float* frfield = nullptr;
+  float* kd = nullptr;                   // derivative k per axis per system, Nyquist = 0
+  float* kk = nullptr;                   // k per axis per system
 
-  // scratch for reductions and host transfers
-  double* red = nullptr;              // partial sums
+  // scratch
+  double* red = nullptr;
   int red_cap = 0;
-  double* sk[TILD_MAX_COMPUTES] = {nullptr};
-  int sk_calls[TILD_MAX_COMPUTES] = {0};
-  float* xfer = nullptr;              // ns*4 floats staging (bead order)
+  float* xfer = nullptr;                 // staging for host transfers, >= 3 * max ns floats
   int* d_status = nullptr;
 
-  cufftHandle plan_r2c = 0, plan_c2r = 0;
-  bool plans = false;
-
-  // spatial sort of the slots (tild_sort.cu)
+  // spatial sort (tild_sort.cu)
   unsigned* sort_keys = nullptr;
   unsigned* sort_keys_alt = nullptr;
   int* sort_vals = nullptr;
   int* sort_perm = nullptr;
   int* sort_newslot = nullptr;
+  int* slot_sys = nullptr;               // system of each slot
   float4* alt_pos[2] = {nullptr, nullptr};
   float* alt_noise = nullptr;
   int* alt_bead_id = nullptr;
@@ -125,21 +178,17 @@ struct tild_ctx {
   void* sort_temp = nullptr;
   size_t sort_temp_bytes = 0;
   int sort_bits = 0;
-  int sort_kg[7] = {0};
-  int sort_interval = 0;               // 0: never
-  int64_t last_sort_step = -1;
+  int sort_cell_bits = 0;
+  int sort_interval = 0;                 // 0: never
+  int64_t steps_since_sort = 0;
   long long sorts = 0;
-  int spread_cap = 0;                  // shared-memory 32-bit words of the tiled spread
-  int spread_kbits = 20;               // fractional bits of the shared 32-bit fixed point
+  int spread_cap = 0;                    // shared-memory 32-bit words of the tiled spread
 
-  // per-stage timing (tild_profile_steps): an event is recorded at every stage boundary
+  // per-stage timing (tild_profile_steps)
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_stage;
   bool profiling = false;
 
-  int64_t step = 0;
-  int64_t forces_step = 0;
-  bool topo_set = false, state_set = false, have_forces = false;
   long long launches = 0;
   std::string err;
 };
@@ -254,15 +303,25 @@ __device__ __forceinline__ void philox_normal3(uint64_t seed, uint32_t bead, int
   z[2] = r1 * c1;
 }
 
+// Ramp multiplier of FFT style k of a system for a force evaluation at `step`
+// (PairStyle::Update, pair_style.cu:347-367: after every update u_k(0) equals
+// A_i + (A_i - A_f) * (step + 1) / max_steps; forces of step n >= 2 see the update of n - 1).
+__host__ __device__ inline float ramp_ratio(const SysDev& d, int k, long long step) {
+  if (!d.sramp[k] || step < 2 || d.max_steps <= 0) return 1.0f;
+  const double Ai = d.sAi[k], Af = d.sAf[k];
+  const double target = Ai + (Ai - Af) * (double)step / (double)d.max_steps;
+  return (float)(target / (double)d.suk0[k]);
+}
+
 // ---- host-side entry points between translation units ------------------------------------
-int tild_build_tables(tild_ctx* c);                   // tild_tables.cu
-int tild_run_forces(tild_ctx* c, int64_t step, bool integrate, float* f_slot);  // tild_step.cu
-int tild_run_spread(tild_ctx* c);                     // tild_step.cu
-int tild_obs_compute(tild_ctx* c, tild_obs* o);       // tild_obs.cu
-int tild_sk_acc_run(tild_ctx* c, int slot, int type);
-int tild_stencil_run(tild_ctx* c, int* inds_dev, float* w_dev);
-int tild_nlist_geom(const tild_ctx* c, float rc, int* nc, float* Lc, int* total, int* cmax);
-int tild_nlist_run(tild_ctx* c, float rc, int group_type, int* cell_of_bead_dev, int* ncount_dev, int* neigh_dev);
+int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
+int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
+int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
+int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
+int tild_stencil_run(tild_ctx* c, int s, int* inds_dev, float* w_dev);
+int tild_nlist_geom(const SysHost& h, float rc, int* nc, float* Lc, int* total, int* cmax);
+int tild_nlist_run(tild_ctx* c, int s, float rc, int group_type, int* cell_of_bead_dev, int* ncount_dev,
+                   int* neigh_dev);
 int tild_check(tild_ctx* c, cudaError_t e, const char* what);
 int tild_check_fft(tild_ctx* c, cufftResult r, const char* what);
 int tild_poll_status(tild_ctx* c);
@@ -270,4 +329,4 @@ int tild_ensure_red(tild_ctx* c, int nvals, int nblocks);
 int tild_sort_alloc(tild_ctx* c);                     // tild_sort.cu
 void tild_sort_free(tild_ctx* c);
 int tild_sort_beads(tild_ctx* c);
-double tild_ramp_ratio(const tild_ctx* c, int fft_slot, int64_t step);
+int tild_upload_sys(tild_ctx* c);                     // tild_api.cu: copies h_sys to d_sys

@@ -102,10 +102,13 @@ __global__ void __launch_bounds__(kObsThreads) k_obs_charge(const float2* __rest
 __global__ void __launch_bounds__(kObsThreads) k_obs_bonds(const float4* __restrict__ pos, const int* __restrict__ bead_id,
                                                           const int* __restrict__ nbr, const int* __restrict__ info,
                                                           const float* __restrict__ bk, const float* __restrict__ br,
-                                                          Geom g, int D, int ns, double* __restrict__ partial) {
+                                                          Geom g, int D, int slot0, int nslot,
+                                                          double* __restrict__ partial) {
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
-    const int in = info[i], nb = in & 3, id1 = bead_id[i];
+  for (int i = slot0 + blockIdx.x * blockDim.x + threadIdx.x; i < slot0 + nslot; i += gridDim.x * blockDim.x) {
+    const int id1 = bead_id[i];
+    if (id1 < 0) continue;
+    const int in = info[i], nb = in & 3;
     const float4 p = pos[i];
     const float x1[3] = {p.x, p.y, p.z};
     for (int b = 0; b < nb; b++) {
@@ -155,10 +158,10 @@ __global__ void k_sk_acc(double2* __restrict__ acc, const float2* __restrict__ r
 
 // stencil export in d_charge_grid order (device_grid_utils.cu:305-339)
 template <int D, int P>
-__global__ void k_stencil(const float4* __restrict__ pos, const int* __restrict__ bead_id, Geom g, int ns,
+__global__ void k_stencil(const float4* __restrict__ pos, const int* __restrict__ bead_id, Geom g, int slot0, int nslot,
                           int* __restrict__ inds, float* __restrict__ wout, int* status) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ns) return;
+  const int i = slot0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slot0 + nslot || bead_id[i] < 0) return;
   const float4 p = pos[i];
   const float xs[3] = {p.x, p.y, p.z};
   float W[3][P + 1];
@@ -203,7 +206,7 @@ __global__ void k_assign_cells(const float4* __restrict__ pos, const int* __rest
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ns) return;
   const float4 p = pos[i];
-  if (group_type >= 0 && tild_type_of(p.w) != group_type) {
+  if (bead_id[i] < 0 || (group_type >= 0 && tild_type_of(p.w) != group_type)) {
     cell_of_slot[i] = -1;
     return;
   }
@@ -241,6 +244,7 @@ __global__ void k_make_nlist(const float4* __restrict__ pos, const int* __restri
   if (i >= ns) return;
   const int cn = cell_of_slot[i];
   const int bid = bead_id[i];
+  if (bid < 0) return;
   if (cn < 0) {
     ncount[bid] = 0;
     return;
@@ -311,7 +315,7 @@ __global__ void k_make_nlist(const float4* __restrict__ pos, const int* __restri
 __global__ void k_scatter_int(const int* __restrict__ src_slot, const int* __restrict__ bead_id, int ns,
                               int* __restrict__ dst_bead) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ns) return;
+  if (i >= ns || bead_id[i] < 0) return;
   dst_bead[bead_id[i]] = src_slot[i];
 }
 
@@ -340,52 +344,56 @@ static int reduce_host(tild_ctx* c, int nvals, int nblocks, double* out) {
   return TILD_OK;
 }
 
-int tild_obs_compute(tild_ctx* c, tild_obs* o) {
+int tild_obs_compute(tild_ctx* c, int si, tild_obs* o) {
+  const SysHost& h = c->sys[si];
+  const SysDev& hd = c->h_sys[si];
   memset(o, 0, sizeof(*o));
-  o->n_styles = c->cfg.n_styles;
-  o->n_p_comps = c->nP;
-  o->step = c->forces_step;
+  o->n_styles = h.cfg.n_styles;
+  o->n_p_comps = h.nP;
+  o->step = h.forces_step;
   const int nblocks = 296;
   if (tild_ensure_red(c, 7, nblocks)) return TILD_ERR_OOM;
-  const float2* rk = reinterpret_cast<const float2*>(c->rhok);
+  const float2* rk = reinterpret_cast<const float2*>(c->rhok) + h.spec0;
   double upe = 0.0;
-  for (size_t s = 0; s < c->styles_k.size(); s++) {
-    const int ci = c->fft_style_cfg[s];
-    const double scale = tild_ramp_ratio(c, (int)s, c->forces_step);
-    k_obs_style<<<nblocks, kObsThreads, 0, c->stream>>>(rk, c->utab + (long long)s * c->g.Mh,
-                                                         reinterpret_cast<const float2*>(c->virk) +
-                                                             (long long)s * c->nP * c->g.Mh,
-                                                         c->styles_k[s].a, c->styles_k[s].b, c->g, c->nP, scale, c->red);
+  for (size_t k = 0; k < h.fft_cfg.size(); k++) {
+    const int ci = h.fft_cfg[k];
+    const double scale = ramp_ratio(hd, (int)k, h.forces_step);
+    k_obs_style<<<nblocks, kObsThreads, 0, c->stream>>>(rk, c->utab + h.utab0 + (long long)k * h.g.Mh,
+                                                         reinterpret_cast<const float2*>(c->virk) + h.virk0 +
+                                                             (long long)k * h.nP * h.g.Mh,
+                                                         hd.sa[k], hd.sb[k], h.g, h.nP, scale, c->red);
     c->launches++;
     double r[7];
     if (reduce_host(c, 7, nblocks, r)) return TILD_ERR_CUDA;
-    o->style_energy[ci] = r[0] * c->dV;
+    o->style_energy[ci] = r[0] * h.dV;
     upe += o->style_energy[ci];
-    for (int j = 0; j < c->nP; j++) {
-      o->style_virial[ci][j] = r[1 + j] * c->dV / c->V / (double)c->D;
+    for (int j = 0; j < h.nP; j++) {
+      o->style_virial[ci][j] = r[1 + j] * h.dV / h.V / (double)h.D;
       o->ptens[j] += o->style_virial[ci][j];
     }
   }
-  if (c->C) {
-    k_obs_charge<<<nblocks, kObsThreads, 0, c->stream>>>(rk + (long long)c->T * c->g.Mh, c->kk, c->g, c->D,
-                                                          (double)c->cfg.bjerrum,
-                                                          (double)c->cfg.smearing * (double)c->cfg.smearing, c->red);
+  if (h.C) {
+    k_obs_charge<<<nblocks, kObsThreads, 0, c->stream>>>(rk + (long long)h.T * h.g.Mh, c->kk + h.kd0, h.g, h.D,
+                                                          (double)h.cfg.bjerrum,
+                                                          (double)h.cfg.smearing * (double)h.cfg.smearing, c->red);
     c->launches++;
     double r[1];
     if (reduce_host(c, 1, nblocks, r)) return TILD_ERR_CUDA;
-    o->uelec = r[0] / (double)c->g.M;
+    o->uelec = r[0] / (double)h.g.M;
     upe += o->uelec;
   }
   {
+    const SysDev* dsys = c->d_sys + si;
     k_obs_bonds<<<nblocks, kObsThreads, 0, c->stream>>>(c->pos[c->cur], c->bead_id, c->bond_nbr, c->bond_info,
-                                                         c->bondk_dev, c->bondr_dev, c->g, c->D, c->ns, c->red);
+                                                         dsys->bond_k, dsys->bond_req, h.g, h.D, h.slot0, h.ns_pad,
+                                                         c->red);
     c->launches++;
     double r[7];
     if (reduce_host(c, 7, nblocks, r)) return TILD_ERR_CUDA;
     o->ubond = r[0];
     upe += o->ubond;
-    for (int j = 0; j < c->nP; j++) {
-      o->bond_vir[j] = r[1 + j] * (1.0 / c->V / (double)c->D);
+    for (int j = 0; j < h.nP; j++) {
+      o->bond_vir[j] = r[1 + j] * (1.0 / h.V / (double)h.D);
       o->ptens[j] += o->bond_vir[j];
     }
   }
@@ -393,43 +401,45 @@ int tild_obs_compute(tild_ctx* c, tild_obs* o) {
   return tild_check(c, cudaGetLastError(), "observables") ? TILD_ERR_CUDA : TILD_OK;
 }
 
-int tild_sk_acc_run(tild_ctx* c, int slot, int type) {
-  if (!c->sk[slot]) {
-    if (tild_check(c, cudaMalloc(&c->sk[slot], sizeof(double2) * c->g.Mh), "alloc sk")) return TILD_ERR_OOM;
-    if (tild_check(c, cudaMemsetAsync(c->sk[slot], 0, sizeof(double2) * c->g.Mh, c->stream), "zero sk"))
+int tild_sk_acc_run(tild_ctx* c, int si, int slot, int type) {
+  SysHost& h = c->sys[si];
+  if (!h.sk[slot]) {
+    if (tild_check(c, cudaMalloc(&h.sk[slot], sizeof(double2) * h.g.Mh), "alloc sk")) return TILD_ERR_OOM;
+    if (tild_check(c, cudaMemsetAsync(h.sk[slot], 0, sizeof(double2) * h.g.Mh, c->stream), "zero sk"))
       return TILD_ERR_CUDA;
-    c->sk_calls[slot] = 0;
+    h.sk_calls[slot] = 0;
   }
-  k_sk_acc<<<nblk(c->g.Mh, 256), 256, 0, c->stream>>>(
-      reinterpret_cast<double2*>(c->sk[slot]), reinterpret_cast<const float2*>(c->rhok) + (long long)type * c->g.Mh,
-      c->g.Mh, 1.0 / (double)c->g.M);
+  k_sk_acc<<<nblk(h.g.Mh, 256), 256, 0, c->stream>>>(
+      reinterpret_cast<double2*>(h.sk[slot]),
+      reinterpret_cast<const float2*>(c->rhok) + h.spec0 + (long long)type * h.g.Mh, h.g.Mh, 1.0 / (double)h.g.M);
   c->launches++;
-  c->sk_calls[slot]++;
+  h.sk_calls[slot]++;
   return tild_check(c, cudaGetLastError(), "sk accumulate") ? TILD_ERR_CUDA : TILD_OK;
 }
 
 template <int D, int P>
-static void launch_stencil(tild_ctx* c, int* inds, float* w) {
-  k_stencil<D, P><<<nblk(c->ns, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->bead_id, c->g, c->ns, inds, w,
-                                                            c->d_status);
+static void launch_stencil(tild_ctx* c, const SysHost& h, int* inds, float* w) {
+  k_stencil<D, P><<<nblk(h.ns_pad, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->bead_id, h.g, h.slot0, h.ns_pad,
+                                                               inds, w, c->d_status);
 }
 
-int tild_stencil_run(tild_ctx* c, int* inds_dev, float* w_dev) {
+int tild_stencil_run(tild_ctx* c, int si, int* inds_dev, float* w_dev) {
+  const SysHost& h = c->sys[si];
   if (c->D == 3) {
-    switch (c->p) {
-      case 0: launch_stencil<3, 0>(c, inds_dev, w_dev); break;
-      case 1: launch_stencil<3, 1>(c, inds_dev, w_dev); break;
-      case 2: launch_stencil<3, 2>(c, inds_dev, w_dev); break;
-      case 3: launch_stencil<3, 3>(c, inds_dev, w_dev); break;
-      default: launch_stencil<3, 4>(c, inds_dev, w_dev); break;
+    switch (c->P) {
+      case 0: launch_stencil<3, 0>(c, h, inds_dev, w_dev); break;
+      case 1: launch_stencil<3, 1>(c, h, inds_dev, w_dev); break;
+      case 2: launch_stencil<3, 2>(c, h, inds_dev, w_dev); break;
+      case 3: launch_stencil<3, 3>(c, h, inds_dev, w_dev); break;
+      default: launch_stencil<3, 4>(c, h, inds_dev, w_dev); break;
     }
   } else {
-    switch (c->p) {
-      case 0: launch_stencil<2, 0>(c, inds_dev, w_dev); break;
-      case 1: launch_stencil<2, 1>(c, inds_dev, w_dev); break;
-      case 2: launch_stencil<2, 2>(c, inds_dev, w_dev); break;
-      case 3: launch_stencil<2, 3>(c, inds_dev, w_dev); break;
-      default: launch_stencil<2, 4>(c, inds_dev, w_dev); break;
+    switch (c->P) {
+      case 0: launch_stencil<2, 0>(c, h, inds_dev, w_dev); break;
+      case 1: launch_stencil<2, 1>(c, h, inds_dev, w_dev); break;
+      case 2: launch_stencil<2, 2>(c, h, inds_dev, w_dev); break;
+      case 3: launch_stencil<2, 3>(c, h, inds_dev, w_dev); break;
+      default: launch_stencil<2, 4>(c, h, inds_dev, w_dev); break;
     }
   }
   c->launches++;
@@ -437,30 +447,35 @@ int tild_stencil_run(tild_ctx* c, int* inds_dev, float* w_dev) {
 }
 
 // NList::Initialize geometry (nlist.cu:85-102) in FP32 as the reference computes it
-int tild_nlist_geom(const tild_ctx* c, float rc, int* nc, float* Lc, int* total, int* cmax) {
+int tild_nlist_geom(const SysHost& h, float rc, int* nc, float* Lc, int* total, int* cmax) {
   float cell_vol = 1.0f, V = 1.0f;
   *total = 1;
   for (int j = 0; j < 3; j++) { nc[j] = 1; Lc[j] = 1.f; }
-  for (int j = 0; j < c->D; j++) {
-    nc[j] = (int)(c->g.L[j] / rc);
+  for (int j = 0; j < h.D; j++) {
+    nc[j] = (int)(h.g.L[j] / rc);
     if (nc[j] < 1) return TILD_ERR_BAD_INPUT;
-    Lc[j] = c->g.L[j] / (int)nc[j];
+    Lc[j] = h.g.L[j] / (int)nc[j];
     *total *= nc[j];
     cell_vol *= Lc[j];
-    V *= c->g.L[j];
+    V *= h.g.L[j];
   }
-  *cmax = (int)((float)(c->ns * cell_vol / V) * 7.5);
+  *cmax = (int)((float)(h.ns * cell_vol / V) * 7.5);
   return TILD_OK;
 }
 
-int tild_nlist_run(tild_ctx* c, float rc, int group_type, int* cell_of_bead_dev, int* ncount_dev, int* neigh_dev) {
+int tild_nlist_run(tild_ctx* c, int si, float rc, int group_type, int* cell_of_bead_dev, int* ncount_dev,
+                   int* neigh_dev) {
+  const SysHost& h = c->sys[si];
   CellGeom cg;
-  cg.D = c->D;
-  if (tild_nlist_geom(c, rc, cg.nc, cg.Lc, &cg.total, &cg.cmax)) return TILD_ERR_BAD_INPUT;
+  cg.D = h.D;
+  if (tild_nlist_geom(h, rc, cg.nc, cg.Lc, &cg.total, &cg.cmax)) return TILD_ERR_BAD_INPUT;
   if (cg.cmax < 1) return TILD_ERR_BAD_INPUT;
   int *cell_of_slot = nullptr, *cnt = nullptr, *cursor = nullptr, *cell_slots = nullptr;
   int rc_ = TILD_OK;
-  if (tild_check(c, cudaMalloc(&cell_of_slot, sizeof(int) * c->ns), "alloc nlist") ||
+  const int n = h.ns_pad;
+  const float4* pos = c->pos[c->cur] + h.slot0;
+  const int* bid = c->bead_id + h.slot0;
+  if (tild_check(c, cudaMalloc(&cell_of_slot, sizeof(int) * n), "alloc nlist") ||
       tild_check(c, cudaMalloc(&cnt, sizeof(int) * cg.total), "alloc nlist") ||
       tild_check(c, cudaMalloc(&cursor, sizeof(int) * cg.total), "alloc nlist") ||
       tild_check(c, cudaMalloc(&cell_slots, sizeof(int) * (size_t)cg.total * cg.cmax), "alloc nlist"))
@@ -468,16 +483,12 @@ int tild_nlist_run(tild_ctx* c, float rc, int group_type, int* cell_of_bead_dev,
   if (rc_ == TILD_OK) {
     cudaMemsetAsync(cnt, 0, sizeof(int) * cg.total, c->stream);
     cudaMemsetAsync(cursor, 0, sizeof(int) * cg.total, c->stream);
-    k_assign_cells<<<nblk(c->ns, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->bead_id, cg, c->ns, group_type,
-                                                            cell_of_slot, cnt);
-    k_fill_cells<<<nblk(c->ns, 256), 256, 0, c->stream>>>(cell_of_slot, c->ns, cursor, cell_slots, cg.cmax,
-                                                          c->d_status);
-    k_make_nlist<<<nblk(c->ns, 256), 256, 0, c->stream>>>(c->pos[c->cur], c->bead_id, cg, c->ns, cell_of_slot, cnt,
-                                                          cell_slots, rc * rc, c->g, ncount_dev, neigh_dev,
-                                                          c->d_status);
+    k_assign_cells<<<nblk(n, 256), 256, 0, c->stream>>>(pos, bid, cg, n, group_type, cell_of_slot, cnt);
+    k_fill_cells<<<nblk(n, 256), 256, 0, c->stream>>>(cell_of_slot, n, cursor, cell_slots, cg.cmax, c->d_status);
+    k_make_nlist<<<nblk(n, 256), 256, 0, c->stream>>>(pos, bid, cg, n, cell_of_slot, cnt, cell_slots, rc * rc, h.g,
+                                                      ncount_dev, neigh_dev, c->d_status);
     c->launches += 3;
-    // cell of each bead in bead order
-    k_scatter_int<<<nblk(c->ns, 256), 256, 0, c->stream>>>(cell_of_slot, c->bead_id, c->ns, cell_of_bead_dev);
+    k_scatter_int<<<nblk(n, 256), 256, 0, c->stream>>>(cell_of_slot, bid, n, cell_of_bead_dev);
     c->launches++;
     if (tild_check(c, cudaStreamSynchronize(c->stream), "nlist")) rc_ = TILD_ERR_CUDA;
   }

@@ -1,5 +1,5 @@
-// tild_step.cu — the per-step hot path: spread -> batched R2C -> k-space multiply -> batched C2R
-// -> fused gather + bonds + integrators.
+// tild_step.cu — the per-step hot path over all systems of an engine: spread -> batched R2C ->
+// k-space multiply -> batched C2R -> fused gather + bonds + integrators.
 //
 // Replaces forces() (forces.cu:42-196) followed by Integrator::Integrate_2()
 // (integrator.cu:24-39).  Differences of formulation, each exact in real arithmetic:
@@ -13,6 +13,7 @@
 //  * the derivative of the Nyquist plane is zero: the reference's Re() of a full C2C inverse
 //    discards exactly those modes;
 //  * stencil weights are recomputed in the gather rather than cached (no ns*S W/inds arrays).
+// Each launch covers every system of the engine: CTAs find their system in a lookup table.
 #include "tild_internal.cuh"
 #include <climits>
 
@@ -20,17 +21,9 @@ namespace {
 
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
-// ---------------------------------------------------------------------------------------------
-// Spreading: d_charge_grid / d_charge_grid_charges (device_grid_utils.cu:111-343)
-// ---------------------------------------------------------------------------------------------
-// Tiled spreading for slot-sorted beads.  One CTA takes 256 consecutive slots; their stencil
-// nodes are accumulated into a shared-memory box (relative to the first bead, periodic offsets
-// folded into [-N/2, N/2]) and the box is added to the global grid once.  Accumulation is in
-// 64-bit fixed point (weight * 2^32, native integer atomics): integer sums do not depend on the
-// order of the additions, so the densities are bitwise reproducible whatever the slot order or
-// the scheduling, and carry ~1e-10 absolute error before the single FP32 rounding.  When the box
-// does not fit (unsorted or widely spread chunks) the CTA adds each node to the global
-// fixed-point grid directly.
+constexpr double kInvFix = 1.0 / 4294967296.0;  // the global accumulator holds 2^32 per unit
+constexpr int kMaxRows = 1024;                  // (y, z) rows of a shared-memory spread box
+
 __device__ __forceinline__ int fold_rel(int r, int N) {
   r %= N;
   if (r < 0) r += N;
@@ -43,16 +36,8 @@ __device__ __forceinline__ int pmod(int n, int N) {
   return n < 0 ? n + N : n;
 }
 
-constexpr double kFix = 4294967296.0;           // 2^32
-constexpr int kMaxRows = 1024;                  // (y, z) rows of a shared-memory spread box
-constexpr double kInvFix = 1.0 / 4294967296.0;
-
-__device__ __forceinline__ unsigned long long to_fix(float v) {
-  return (unsigned long long)__double2ll_rn((double)v * kFix);
-}
-
 // Chunk bounding box of the beads' stencil bases, relative to the chunk's first bead.
-// Returns false when no bead of the chunk is finite.  Every thread of the block must call it.
+// Returns false when no bead of the chunk is valid.  Every thread of the block must call it.
 template <int D, int P>
 __device__ __forceinline__ bool chunk_box(bool ok, const int (&rel)[3], int* s_min, int* s_max, int (&mn)[3],
                                           int (&ext)[3], long long& vol) {
@@ -84,10 +69,11 @@ __device__ __forceinline__ void chunk_origin(const float4* __restrict__ pos, int
   if (threadIdx.x == 0) {
     const float4 p0 = pos[i0];
     const float x0[3] = {p0.x, p0.y, p0.z};
+    const bool valid = tild_type_of(p0.w) != kPadType;
     float Wd[P + 1];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      s_g0[d] = (d < D && isfinite(x0[d])) ? axis_base<P>(x0[d], g.dx[d], Wd) : 0;
+      s_g0[d] = (valid && d < D && isfinite(x0[d])) ? axis_base<P>(x0[d], g.dx[d], Wd) : 0;
       s_min[d] = INT_MAX;
       s_max[d] = INT_MIN;
     }
@@ -95,15 +81,31 @@ __device__ __forceinline__ void chunk_origin(const float4* __restrict__ pos, int
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------------------------
+// Spreading: d_charge_grid / d_charge_grid_charges (device_grid_utils.cu:111-343)
+// ---------------------------------------------------------------------------------------------
+// One CTA takes 256 consecutive slots of one system; their stencil nodes are accumulated into a
+// shared-memory box (relative to the first bead, periodic offsets folded into [-N/2, N/2]) and
+// the box is added to the global grid once.  Accumulation is fixed point: the shared box holds
+// 32-bit integers with 2^kbits per unit (native integer atomics; kbits is chosen per system so
+// 256 beads at the largest weight cannot overflow), the global accumulator 64-bit integers with
+// 2^32 per unit.  Integer sums do not depend on the order of the additions, so the densities are
+// bitwise reproducible whatever the slot order or scheduling.  A chunk whose box does not fit
+// adds each node to the global accumulator directly.
 template <int D, int P>
 __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__ pos, const float* __restrict__ charge,
-                                                     int ns, Geom g, unsigned long long* __restrict__ rho_fx, int T,
-                                                     int C, int cap, int kbits, int* status) {
-  // shared box: 32-bit fixed point with 2^kbits per unit (native integer shared atomics); kbits is
-  // chosen per context so that 256 beads at the largest weight cannot overflow
+                                                     const int* __restrict__ cta_sys,
+                                                     const SysDev* __restrict__ sysd,
+                                                     unsigned long long* __restrict__ rho_fx_all, int cap,
+                                                     int* status) {
   extern __shared__ int smi[];
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ long long s_row[kMaxRows];
+  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
+  if (!sd.active) return;
+  const Geom g = sd.g;
+  const int T = sd.T, C = sd.C, kbits = sd.kbits;
+  unsigned long long* rho_fx = rho_fx_all + sd.grid0;
   const int i0 = blockIdx.x * blockDim.x;
   const int i = i0 + threadIdx.x;
   chunk_origin<D, P>(pos, i0, g, s_g0, s_min, s_max);
@@ -112,17 +114,19 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   int t = 0;
   float q = 0.f;
   bool ok = false;
-  if (i < ns) {
+  {
     const float4 p = pos[i];
     const float xs[3] = {p.x, p.y, p.z};
-    ok = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
-    if (!ok) {
-      atomicOr(status, ST_NONFINITE_POS);
-    } else {
-      t = tild_type_of(p.w);
-      q = C ? charge[i] : 0.f;
+    t = tild_type_of(p.w);
+    if (t != kPadType) {
+      ok = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
+      if (!ok) {
+        atomicOr(status, ST_NONFINITE_POS);
+      } else {
+        q = C ? charge[i] : 0.f;
 #pragma unroll
-      for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
+        for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
+      }
     }
   }
   int mn[3], ext[3];
@@ -203,23 +207,25 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
       for (int a = 0; a <= P; a++) idx[d][a] = pmod(s_g0[d] + rel[d] + a, g.nx[d]);
     unsigned long long* rt = rho_fx + (long long)t * M;
     unsigned long long* rc = rho_fx + (long long)T * M;
+    const double sc64 = 4294967296.0 / (double)g.gvol;
 #pragma unroll
     for (int ix = 0; ix <= P; ix++)
 #pragma unroll
       for (int iy = 0; iy <= P; iy++) {
         const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
-        const float wxy = W[0][ix] * W[1][iy] * ig;
+        const float wxy = W[0][ix] * W[1][iy];
         if (D == 3) {
 #pragma unroll
           for (int iz = 0; iz <= P; iz++) {
             const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
-            const float W3 = wxy * W[2][iz];
-            atomicAdd(rt + m, to_fix(W3));
-            if (qc) atomicAdd(rc + m, to_fix(W3 * q));
+            const double W3 = (double)(wxy * W[2][iz]) * sc64;
+            atomicAdd(rt + m, (unsigned long long)__double2ll_rn(W3));
+            if (qc) atomicAdd(rc + m, (unsigned long long)__double2ll_rn(W3 * q));
           }
         } else {
-          atomicAdd(rt + row, to_fix(wxy));
-          if (qc) atomicAdd(rc + row, to_fix(wxy * q));
+          const double W3 = (double)wxy * sc64;
+          atomicAdd(rt + row, (unsigned long long)__double2ll_rn(W3));
+          if (qc) atomicAdd(rc + row, (unsigned long long)__double2ll_rn(W3 * q));
         }
       }
   }
@@ -238,19 +244,22 @@ __global__ void k_fix_to_float(unsigned long long* __restrict__ fx, float* __res
 // k-space multiply (replaces d_prepareForceKSpace, device_array_utils.cu:298-312, for every
 // style and side, and d_prepareElectrostaticPotential / d_prepareElectricField :199-241)
 // ---------------------------------------------------------------------------------------------
-struct KArgs {
-  int nstyle;
-  int a[TILD_MAX_STYLES];
-  int b[TILD_MAX_STYLES];
-  float scale[TILD_MAX_STYLES];
-};
-
 template <int D, int NT>
-__global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok, float2* __restrict__ gk,
-                                             const float* __restrict__ utab, const float* __restrict__ ctab,
-                                             const float* __restrict__ kd, Geom g, int T, int C, KArgs ka) {
-  const long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (h >= g.Mh) return;
+__global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_all, float2* __restrict__ gk_all,
+                                             const float* __restrict__ utab_all, const float* __restrict__ ctab_all,
+                                             const float* __restrict__ kd_all, const int* __restrict__ cta_sys,
+                                             const int* __restrict__ blk0, const SysDev* __restrict__ sysd,
+                                             int integrate) {
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  const Geom& g = sd.g;
+  const long long h = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
+  const long long Mh = g.Mh;
+  if (h >= Mh) return;
+  const int T = sd.T, C = sd.C;
+  const float2* rhok = rhok_all + sd.spec0;
+  float2* gk = gk_all + sd.spec0 * D;
+  const float* kd = kd_all + sd.kd0;
   const int ix = (int)(h % g.nxh);
   const long long r = h / g.nxh;
   const int iy = (int)(r % g.nx[1]);
@@ -259,74 +268,58 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok, f
   kv[0] = kd[ix];
   kv[1] = kd[g.nx[0] + iy];
   kv[2] = (D == 3) ? kd[g.nx[0] + g.nx[1] + iz] : 0.f;
-  const long long Mh = g.Mh;
-  float2 rk[NT], phi[NT];
+  const long long est = sd.step + (integrate ? 1 : 0);
+  if (NT > 0) {
+    constexpr int NA = NT > 0 ? NT : 1;
+    float2 rk[NA], phi[NA];
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
-    rk[t] = (t < T) ? rhok[(long long)t * Mh + h] : make_float2(0.f, 0.f);
-    phi[t] = make_float2(0.f, 0.f);
-  }
-  for (int s = 0; s < ka.nstyle; s++) {
-    const float u = utab[(long long)s * Mh + h] * ka.scale[s];
-    const int a = ka.a[s], b = ka.b[s];
-    // explicit selects keep rk[] and phi[] in registers
-    float2 ra = make_float2(0.f, 0.f), rb = make_float2(0.f, 0.f);
+    for (int t = 0; t < NA; t++) {
+      rk[t] = (t < T) ? rhok[(long long)t * Mh + h] : make_float2(0.f, 0.f);
+      phi[t] = make_float2(0.f, 0.f);
+    }
+    for (int k = 0; k < sd.nfft; k++) {
+      const float u = utab_all[sd.utab0 + (long long)k * Mh + h] * ramp_ratio(sd, k, est);
+      const int a = sd.sa[k], b = sd.sb[k];
+      // explicit selects keep rk[] and phi[] in registers
+      float2 ra = make_float2(0.f, 0.f), rb = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int t = 0; t < NT; t++) {
-      if (t == a) ra = rk[t];
-      if (t == b) rb = rk[t];
+      for (int t = 0; t < NA; t++) {
+        if (t == a) ra = rk[t];
+        if (t == b) rb = rk[t];
+      }
+#pragma unroll
+      for (int t = 0; t < NA; t++) {
+        if (t == a) { phi[t].x += u * rb.x; phi[t].y += u * rb.y; }
+        if (t == b) { phi[t].x += u * ra.x; phi[t].y += u * ra.y; }
+      }
     }
 #pragma unroll
-    for (int t = 0; t < NT; t++) {
-      if (t == a) { phi[t].x += u * rb.x; phi[t].y += u * rb.y; }
-      if (t == b) { phi[t].x += u * ra.x; phi[t].y += u * ra.y; }
+    for (int t = 0; t < NA; t++) {
+      if (t >= T) break;
+#pragma unroll
+      for (int d = 0; d < D; d++)  // -i k_d Phi
+        gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
     }
-  }
-#pragma unroll
-  for (int t = 0; t < NT; t++) {
-    if (t >= T) break;
-#pragma unroll
-    for (int d = 0; d < D; d++)  // -i k_d Phi
-      gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
+  } else {  // more types than the specialised kernels cover: same arithmetic, local arrays
+    float2 phi[TILD_MAX_TYPES];
+    for (int t = 0; t < T; t++) phi[t] = make_float2(0.f, 0.f);
+    for (int k = 0; k < sd.nfft; k++) {
+      const float u = utab_all[sd.utab0 + (long long)k * Mh + h] * ramp_ratio(sd, k, est);
+      const int a = sd.sa[k], b = sd.sb[k];
+      const float2 ra = rhok[(long long)a * Mh + h], rb = rhok[(long long)b * Mh + h];
+      phi[a].x += u * rb.x; phi[a].y += u * rb.y;
+      phi[b].x += u * ra.x; phi[b].y += u * ra.y;
+    }
+    for (int t = 0; t < T; t++)
+      for (int d = 0; d < D; d++)
+        gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
   }
   if (C) {
     const float2 rc = rhok[(long long)T * Mh + h];
-    const float cm = ctab[h];
+    const float cm = ctab_all[sd.ctab0 + h];
     const float2 pc = make_float2(cm * rc.x, cm * rc.y);
 #pragma unroll
     for (int d = 0; d < D; d++) gk[((long long)T * D + d) * Mh + h] = make_float2(kv[d] * pc.y, -kv[d] * pc.x);
-  }
-}
-
-// Generic channel count (T > TILD_MAXT_FAST): same arithmetic with local arrays.
-template <int D>
-__global__ void k_kmul_generic(const float2* __restrict__ rhok, float2* __restrict__ gk, const float* __restrict__ utab,
-                               const float* __restrict__ ctab, const float* __restrict__ kd, Geom g, int T, int C,
-                               KArgs ka) {
-  const long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (h >= g.Mh) return;
-  const int ix = (int)(h % g.nxh);
-  const long long r = h / g.nxh;
-  const int iy = (int)(r % g.nx[1]);
-  const int iz = (int)(r / g.nx[1]);
-  float kv[3] = {kd[ix], kd[g.nx[0] + iy], (D == 3) ? kd[g.nx[0] + g.nx[1] + iz] : 0.f};
-  const long long Mh = g.Mh;
-  float2 phi[TILD_MAX_TYPES];
-  for (int t = 0; t < T; t++) phi[t] = make_float2(0.f, 0.f);
-  for (int s = 0; s < ka.nstyle; s++) {
-    const float u = utab[(long long)s * Mh + h] * ka.scale[s];
-    const int a = ka.a[s], b = ka.b[s];
-    const float2 ra = rhok[(long long)a * Mh + h], rb = rhok[(long long)b * Mh + h];
-    phi[a].x += u * rb.x; phi[a].y += u * rb.y;
-    phi[b].x += u * ra.x; phi[b].y += u * ra.y;
-  }
-  for (int t = 0; t < T; t++)
-    for (int d = 0; d < D; d++) gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
-  if (C) {
-    const float2 rc = rhok[(long long)T * Mh + h];
-    const float cm = ctab[h];
-    for (int d = 0; d < D; d++)
-      gk[((long long)T * D + d) * Mh + h] = make_float2(kv[d] * cm * rc.y, -kv[d] * cm * rc.x);
   }
 }
 
@@ -343,35 +336,31 @@ __global__ void k_fieldphase_apply(float* __restrict__ gfield, const float* __re
   }
 }
 
-// ---------------------------------------------------------------------------------------------
-// Gather + bonds + integrators (d_add_grid_forces{2D,3D}, d_add_grid_forces_charges_*,
-// device_grid_utils.cu:346-452; d_bonds, device_bonds.cu:4-60; d_GJF_integrator,
-// device_GJF_integrator.cu:4-62; d_EM_integrator, device_EM_integrator.cu:5-36)
-// ---------------------------------------------------------------------------------------------
-struct GArgs {
-  int64_t step;
-  uint64_t seed;
-  float delt, noise_mag;
-  int n_integ;
-  int integ_kind[TILD_MAX_INTEGRATORS];
-  int type_mask[TILD_MAX_TYPES];
-  float mass[TILD_MAX_TYPES];
-  float diff[TILD_MAX_TYPES];
-  float bond_k[TILD_MAX_BOND_TYPES];
-  float bond_req[TILD_MAX_BOND_TYPES];
-};
-
 // Interleave the C2R output [(T+C)][D][M] into one float4 (-dPhi/dx, -dPhi/dy, -dPhi/dz, 0) per
 // grid point and channel, so the gather reads a stencil node with a single 16-byte load.
-__global__ void k_interleave(const float* __restrict__ planar, float4* __restrict__ g4, int nch, int D, long long M) {
-  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+template <int D>
+__global__ void k_interleave(const float* __restrict__ planar_all, float4* __restrict__ g4_all,
+                             const int* __restrict__ cta_sys, const int* __restrict__ blk0,
+                             const SysDev* __restrict__ sysd) {
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  const long long M = sd.g.M;
+  const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
   if (m >= M) return;
+  const float* planar = planar_all + sd.grid0 * D;
+  float4* g4 = g4_all + sd.grid0;
+  const int nch = sd.T + sd.C;
   for (int ch = 0; ch < nch; ch++) {
     const float* src = planar + (long long)ch * D * M + m;
     g4[(long long)ch * M + m] = make_float4(src[0], src[M], D == 3 ? src[2 * M] : 0.f, 0.f);
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Gather + bonds + integrators (d_add_grid_forces{2D,3D}, d_add_grid_forces_charges_*,
+// device_grid_utils.cu:346-452; d_bonds, device_bonds.cu:4-60; d_GJF_integrator,
+// device_GJF_integrator.cu:4-62; d_EM_integrator, device_EM_integrator.cu:5-36)
+// ---------------------------------------------------------------------------------------------
 template <int D, int P>
 __device__ __forceinline__ void gather4(const float4* __restrict__ F, const float (&W)[3][P + 1],
                                         const int (&idx)[3][P + 1], const Geom& g, float (&acc)[3]) {
@@ -399,22 +388,28 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ F, const floa
 }
 
 template <int D, int P, bool INTEG, bool XW>
-__global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(const float4* __restrict__ pos_in, float4* __restrict__ pos_io,
-                                                  float* __restrict__ noise, const int* __restrict__ bead_id,
-                                                  const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
-                                                  const float* __restrict__ charge, const float4* __restrict__ g4,
-                                                  Geom g, int T, int C, GArgs ga, float* __restrict__ f_out,
-                                                  curandStateXORWOW_t* __restrict__ xw, int ns, int* status) {
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(
+    const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
+    const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
+    const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
+    const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
+    int* status) {
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  if (!sd.active) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ns) return;
   const float4 p = pos_in[i];
+  const int t = tild_type_of(p.w);
+  if (t == kPadType) return;
   float x[3] = {p.x, p.y, p.z};
   if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
     atomicOr(status, ST_NONFINITE_POS);
     return;  // left in place; the host reports TILD_ERR_NAN
   }
-  const int t = tild_type_of(p.w);
+  const Geom& g = sd.g;
   const long long M = g.M;
+  const int T = sd.T, C = sd.C;
+  const float4* g4 = g4_all + sd.grid0;
   float f[3] = {0.f, 0.f, 0.f};
   {
     float W[3][P + 1];
@@ -455,47 +450,48 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(const float4* 
     float mf = 0.f;
     if (mdr2 > 1.0E-4f) {
       const float mdr = sqrtf(mdr2);
-      mf = 2.0f * ga.bond_k[bt] * (mdr - ga.bond_req[bt]) / mdr;
+      mf = 2.0f * sd.bond_k[bt] * (mdr - sd.bond_req[bt]) / mdr;
     }
 #pragma unroll
     for (int d = 0; d < D; d++) f[d] -= mf * dr[d];
   }
   const int bid = bead_id[i];
-  if (f_out) {
+  if (f_out && s == f_sys) {
 #pragma unroll
     for (int d = 0; d < D; d++) f_out[(long long)bid * D + d] = f[d];
   }
   if (!INTEG) return;
   // integrators in input order (integrator.cu:24-39 is called for each in turn)
-  const int mask = ga.type_mask[t];
+  const int mask = sd.type_mask[t];
+  const long long est = sd.step + 1;
   const float4 po = pos_io[i];  // x_{n-1} (GJF xo)
   float xo[3] = {po.x, po.y, po.z};
   float on[3] = {0.f, 0.f, 0.f};
   bool any_gjf = false;
   curandStateXORWOW_t st;
   if (XW && mask) st = xw[i];
-  for (int ig = 0; ig < ga.n_integ; ig++) {
+  for (int ig = 0; ig < sd.n_integ; ig++) {
     if (!(mask & (1 << ig))) continue;
     float z[3];
     if (XW) {
 #pragma unroll
       for (int d = 0; d < D; d++) z[d] = curand_normal(&st);
     } else {
-      philox_normal3(ga.seed, (uint32_t)bid, ga.step, (uint32_t)ig, z);
+      philox_normal3(sd.seed, (uint32_t)bid, est, (uint32_t)ig, z);
     }
-    if (ga.integ_kind[ig] == TILD_INTEGRATOR_GJF) {
+    if (sd.integ_kind[ig] == TILD_INTEGRATOR_GJF) {
       if (!any_gjf) {
 #pragma unroll
         for (int d = 0; d < D; d++) on[d] = noise[3 * (long long)i + d];
         any_gjf = true;
       }
-      const float m = ga.mass[t], df = ga.diff[t], delt = ga.delt;
+      const float m = sd.mass[t], df = sd.diff[t], delt = sd.delt;
       const float b = m / (m + delt / (2.0f * df));
       const float a = (1.0f - delt / (2.0f * df * m)) / (1.0f + delt / (2.0f * df * m));
       const float delt2 = delt * delt;
 #pragma unroll
       for (int d = 0; d < D; d++) {
-        const float nn = ga.noise_mag / df * z[d];
+        const float nn = sd.noise_mag / df * z[d];
         const float xtmp = x[d];
         if (xo[d] - x[d] > g.L[d] / 2.0f) xo[d] -= g.L[d];
         else if (xo[d] - x[d] < -g.L[d] / 2.0f) xo[d] += g.L[d];
@@ -509,7 +505,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(const float4* 
     } else {
 #pragma unroll
       for (int d = 0; d < D; d++) {
-        float xn = x[d] + ga.delt * f[d] + ga.noise_mag * z[d];
+        float xn = x[d] + sd.delt * f[d] + sd.noise_mag * z[d];
         if (xn > g.L[d]) xn -= g.L[d];
         else if (xn < 0.0) xn += g.L[d];
         x[d] = xn;
@@ -524,36 +520,49 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(const float4* 
   }
 }
 
+// inactive systems keep their slots: copy x_n into the rotated buffer so their state survives
+__global__ void k_hold_inactive(const float4* __restrict__ pos_in, float4* __restrict__ pos_io,
+                                const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd) {
+  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
+  if (sd.active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  pos_io[i] = pos_in[i];
+}
+
+__global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys && sysd[s].active) sysd[s].step += 1;
+}
+
 template <int D, int P>
 void launch_spread(tild_ctx* c) {
   const size_t smem = sizeof(int) * (size_t)c->spread_cap;
   cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_spread_tiled<D, P><<<nblk(c->ns, 256), 256, smem, c->stream>>>(c->pos[c->cur], c->charge, c->ns, c->g, c->rho_fx,
-                                                                    c->T, c->C, c->spread_cap, c->spread_kbits,
-                                                                    c->d_status);
+  k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
+                                                                   c->rho_fx, c->spread_cap, c->d_status);
 }
 
 template <int D, int P, bool I, bool X>
-void launch_gather_k(tild_ctx* c, const GArgs& ga, float* f_out) {
-  k_gather<D, P, I, X><<<nblk(c->ns, 256), 256, 0, c->stream>>>(
-      c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4, c->g,
-      c->T, c->C, ga, f_out, c->xorwow, c->ns, c->d_status);
+void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
+  k_gather<D, P, I, X><<<c->n_cta_bead, kTile, 0, c->stream>>>(
+      c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
+      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->d_status);
 }
 
 template <int D, int P>
-void launch_gather(tild_ctx* c, const GArgs& ga, bool integ, float* f_out) {
-  const bool xw = c->cfg.rng == TILD_RNG_XORWOW;
+void launch_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
+  const bool xw = c->rng == TILD_RNG_XORWOW;
   if (integ) {
-    if (xw) launch_gather_k<D, P, true, true>(c, ga, f_out);
-    else launch_gather_k<D, P, true, false>(c, ga, f_out);
+    if (xw) launch_gather_k<D, P, true, true>(c, f_out, f_sys);
+    else launch_gather_k<D, P, true, false>(c, f_out, f_sys);
   } else {
-    launch_gather_k<D, P, false, false>(c, ga, f_out);
+    launch_gather_k<D, P, false, false>(c, f_out, f_sys);
   }
 }
 
 template <int D>
 void dispatch_p_spread(tild_ctx* c) {
-  switch (c->p) {
+  switch (c->P) {
     case 0: launch_spread<D, 0>(c); break;
     case 1: launch_spread<D, 1>(c); break;
     case 2: launch_spread<D, 2>(c); break;
@@ -563,108 +572,98 @@ void dispatch_p_spread(tild_ctx* c) {
 }
 
 template <int D>
-void dispatch_p_gather(tild_ctx* c, const GArgs& ga, bool integ, float* f_out) {
-  switch (c->p) {
-    case 0: launch_gather<D, 0>(c, ga, integ, f_out); break;
-    case 1: launch_gather<D, 1>(c, ga, integ, f_out); break;
-    case 2: launch_gather<D, 2>(c, ga, integ, f_out); break;
-    case 3: launch_gather<D, 3>(c, ga, integ, f_out); break;
-    default: launch_gather<D, 4>(c, ga, integ, f_out); break;
+void dispatch_p_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
+  switch (c->P) {
+    case 0: launch_gather<D, 0>(c, integ, f_out, f_sys); break;
+    case 1: launch_gather<D, 1>(c, integ, f_out, f_sys); break;
+    case 2: launch_gather<D, 2>(c, integ, f_out, f_sys); break;
+    case 3: launch_gather<D, 3>(c, integ, f_out, f_sys); break;
+    default: launch_gather<D, 4>(c, integ, f_out, f_sys); break;
   }
 }
 
 template <int D>
-void launch_kmul(tild_ctx* c, const KArgs& ka) {
-  const unsigned nb = nblk(c->g.Mh, 256);
+void launch_kmul(tild_ctx* c, bool integ) {
   const float2* rk = reinterpret_cast<const float2*>(c->rhok);
   float2* gk = reinterpret_cast<float2*>(c->gk);
-  switch (c->T) {
-    case 1: k_kmul<D, 1><<<nb, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->g, c->T, c->C, ka); break;
-    case 2: k_kmul<D, 2><<<nb, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->g, c->T, c->C, ka); break;
-    case 3: k_kmul<D, 3><<<nb, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->g, c->T, c->C, ka); break;
-    case 4: k_kmul<D, 4><<<nb, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->g, c->T, c->C, ka); break;
-    default: k_kmul_generic<D><<<nb, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->g, c->T, c->C, ka); break;
+  int* blk0 = c->cta_spec + c->n_cta_spec;  // first-block table stored after the lookup table
+  const int n = c->n_cta_spec;
+  switch (c->maxT) {
+    case 1: k_kmul<D, 1><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
+    case 2: k_kmul<D, 2><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
+    case 3: k_kmul<D, 3><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
+    case 4: k_kmul<D, 4><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
+    default: k_kmul<D, 0><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
   }
 }
 
 }  // namespace
 
-int tild_run_spread(tild_ctx* c) {
-  // the fixed-point accumulator is all zeros here: it starts zeroed and k_fix_to_float clears it
-  tild_mark(c, STAGE_SPREAD);
-  if (c->D == 3) dispatch_p_spread<3>(c);
-  else dispatch_p_spread<2>(c);
-  c->launches++;
-  tild_mark(c, STAGE_ZERO);
-  const long long n = (long long)(c->T + c->C) * c->g.M;
-  k_fix_to_float<<<nblk(n, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, n);
-  c->launches++;
-  return tild_check(c, cudaGetLastError(), "spread") ? TILD_ERR_CUDA : TILD_OK;
-}
-
-int tild_run_forces(tild_ctx* c, int64_t step, bool integrate, float* f_bead) {
-  if (integrate && c->sort_interval > 0 && step - 1 - c->last_sort_step >= c->sort_interval) {
+int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
+  if (integrate && c->sort_interval > 0 && c->steps_since_sort >= c->sort_interval) {
     tild_mark(c, STAGE_SORT);
     int rs = tild_sort_beads(c);
     if (rs) return rs;
   }
-  int rc = tild_run_spread(c);
-  if (rc) return rc;
+  tild_mark(c, STAGE_SPREAD);
+  if (c->D == 3) dispatch_p_spread<3>(c);
+  else dispatch_p_spread<2>(c);
+  tild_mark(c, STAGE_ZERO);
+  k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
+  c->launches += 2;
+  if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
-  if (tild_check_fft(c, cufftExecR2C(c->plan_r2c, c->rho, c->rhok), "R2C")) return TILD_ERR_CUDA;
-  if (c->T > 0 && (c->styles_k.size() > 0 || c->C)) {
-    KArgs ka;
-    ka.nstyle = (int)c->styles_k.size();
-    for (int s = 0; s < ka.nstyle; s++) {
-      ka.a[s] = c->styles_k[s].a;
-      ka.b[s] = c->styles_k[s].b;
-      ka.scale[s] = (float)tild_ramp_ratio(c, s, step);
-    }
-    tild_mark(c, STAGE_KMUL);
-    if (c->D == 3) launch_kmul<3>(c, ka);
-    else launch_kmul<2>(c, ka);
-    c->launches++;
-    if (tild_check(c, cudaGetLastError(), "kmul")) return TILD_ERR_CUDA;
-    tild_mark(c, STAGE_C2R);
-    if (tild_check_fft(c, cufftExecC2R(c->plan_c2r, c->gk, c->gfield), "C2R")) return TILD_ERR_CUDA;
-  } else {
-    if (tild_check(c, cudaMemsetAsync(c->gfield, 0, sizeof(float) * (size_t)(c->T + c->C) * c->D * c->g.M, c->stream),
-                   "zero field"))
+  for (auto& b : c->buckets)
+    if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+  tild_mark(c, STAGE_KMUL);
+  if (c->D == 3) launch_kmul<3>(c, integrate);
+  else launch_kmul<2>(c, integrate);
+  c->launches++;
+  if (tild_check(c, cudaGetLastError(), "kmul")) return TILD_ERR_CUDA;
+  tild_mark(c, STAGE_C2R);
+  for (auto& b : c->buckets)
+    if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
       return TILD_ERR_CUDA;
-  }
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
-  for (size_t fi = 0; fi < c->fields.size(); fi++) {
-    k_fieldphase_apply<<<nblk(c->g.M, 256), 256, 0, c->stream>>>(c->gfield, c->rho,
-                                                                 c->frfield + (long long)fi * c->D * c->g.M,
-                                                                 c->fields[fi].a, c->fields[fi].b, c->D, c->g.M);
+  for (const FieldK& fk : c->fields) {
+    const SysHost& h = c->sys[fk.sys];
+    k_fieldphase_apply<<<nblk(h.g.M, 256), 256, 0, c->stream>>>(c->gfield + h.grid0 * c->D, c->rho + h.grid0,
+                                                                 c->frfield + fk.fr0, fk.a, fk.b, c->D, h.g.M);
     c->launches++;
-  }
-  GArgs ga;
-  memset(&ga, 0, sizeof(ga));
-  ga.step = step;
-  ga.seed = c->cfg.seed;
-  ga.delt = c->cfg.delt;
-  ga.noise_mag = c->cfg.noise_mag;
-  ga.n_integ = c->cfg.n_integrators;
-  for (int k = 0; k < ga.n_integ; k++) ga.integ_kind[k] = c->cfg.integrators[k].kind;
-  for (int t = 0; t < c->T; t++) {
-    ga.type_mask[t] = c->type_integ_mask[t];
-    ga.mass[t] = c->cfg.mass[t];
-    ga.diff[t] = c->cfg.diff[t];
-  }
-  for (int b = 0; b < c->cfg.n_bond_types; b++) {
-    ga.bond_k[b] = c->cfg.bond_k[b];
-    ga.bond_req[b] = c->cfg.bond_req[b];
   }
   tild_mark(c, STAGE_GATHER);
-  k_interleave<<<nblk(c->g.M, 256), 256, 0, c->stream>>>(c->gfield, c->g4, c->T + c->C, c->D, c->g.M);
-  c->launches++;
-  if (c->D == 3) dispatch_p_gather<3>(c, ga, integrate, f_bead);
-  else dispatch_p_gather<2>(c, ga, integrate, f_bead);
+  {
+    int* blk0 = c->cta_grid + c->n_cta_grid;
+    if (c->D == 3) k_interleave<3><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
+    else k_interleave<2><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
+    c->launches++;
+  }
+  if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys);
+  else dispatch_p_gather<2>(c, integrate, f_bead, f_sys);
   c->launches++;
   if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
-  if (integrate) c->cur ^= 1;
-  c->forces_step = step;
-  c->have_forces = true;
+  if (integrate) {
+    bool any_inactive = false;
+    for (const SysHost& h : c->sys) any_inactive |= !h.active;
+    if (any_inactive) {
+      k_hold_inactive<<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->pos[c->cur ^ 1], c->cta_bead,
+                                                               c->d_sys);
+      c->launches++;
+    }
+    k_advance_steps<<<nblk(c->nsys, 128), 128, 0, c->stream>>>(c->d_sys, c->nsys);
+    c->launches++;
+    c->cur ^= 1;
+    c->steps_since_sort++;
+  }
+  for (int s = 0; s < c->nsys; s++) {
+    SysHost& h = c->sys[s];
+    if (!h.active) continue;
+    if (integrate) {
+      h.step++;
+      c->h_sys[s].step = h.step;
+    }
+    h.forces_step = h.step;
+    h.have_forces = true;
+  }
   return TILD_OK;
 }

@@ -206,11 +206,12 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
 
-int tild_build_tables(tild_ctx* c) {
-  const Geom& g = c->g;
-  const int D = c->D;
+int tild_build_tables(tild_ctx* c, int si) {
+  SysHost& h = c->sys[si];
+  const Geom& g = h.g;
+  const int D = h.D;
   const double invM = 1.0 / (double)g.M;
-  const int ref = c->cfg.table_mode == TILD_TABLES_REF_FP32;
+  const int ref = h.cfg.table_mode == TILD_TABLES_REF_FP32;
   cudaStream_t st = c->stream;
 
   // per-axis k values: kk for k^2 (reference convention), kd for derivatives (Nyquist = 0)
@@ -226,12 +227,12 @@ int tild_build_tables(tild_ctx* c) {
       }
       off += g.nx[d];
     }
-    if (tild_check(c, cudaMemcpyAsync(c->kk, kk.data(), kk.size() * 4, cudaMemcpyHostToDevice, st), "copy k")) return TILD_ERR_CUDA;
-    if (tild_check(c, cudaMemcpyAsync(c->kd, kd.data(), kd.size() * 4, cudaMemcpyHostToDevice, st), "copy kd")) return TILD_ERR_CUDA;
+    if (tild_check(c, cudaMemcpyAsync(c->kk + h.kd0, kk.data(), kk.size() * 4, cudaMemcpyHostToDevice, st), "copy k")) return TILD_ERR_CUDA;
+    if (tild_check(c, cudaMemcpyAsync(c->kd + h.kd0, kd.data(), kd.size() * 4, cudaMemcpyHostToDevice, st), "copy kd")) return TILD_ERR_CUDA;
     if (tild_check(c, cudaStreamSynchronize(st), "sync k")) return TILD_ERR_CUDA;
   }
 
-  const int nfft = (int)c->styles_k.size();
+  const int nfft = (int)h.fft_cfg.size();
   // per-direction real slabs start on 16-byte boundaries (cuFFT rejects a misaligned output)
   const long long Mpad = (g.M + 1) / 2 * 2;
   double* ufull = nullptr;
@@ -259,8 +260,9 @@ int tild_build_tables(tild_ctx* c) {
          tild_check_fft(c, cufftSetStream(pd2z, st), "stream d2z")))
       rc = TILD_ERR_CUDA;
   }
+  SysDev& hd = c->h_sys[si];
   for (int s = 0; s < nfft && rc == TILD_OK; s++) {
-    const tild_pair_style& ps = c->cfg.styles[c->fft_style_cfg[s]];
+    const tild_pair_style& ps = h.cfg.styles[h.fft_cfg[s]];
     StyleParams sp;
     sp.kind = ps.style;
     sp.A = ps.prefactor;
@@ -269,12 +271,12 @@ int tild_build_tables(tild_ctx* c) {
     sp.Af = ps.prefactor;
     sp.sig2f = (float)sp.sig2;
     sp.Rf = ps.rp;
-    k_style_table<<<nblk(g.Mh, 256), 256, 0, st>>>(c->utab + (long long)s * g.Mh, ufull, sp, g, D, ref, invM);
+    k_style_table<<<nblk(g.Mh, 256), 256, 0, st>>>(c->utab + h.utab0 + (long long)s * g.Mh, ufull, sp, g, D, ref, invM);
     c->launches++;
     double u0 = 0.0;
     if (tild_check(c, cudaMemcpyAsync(&u0, ufull, sizeof(double), cudaMemcpyDeviceToHost, st), "u0") ||
         tild_check(c, cudaStreamSynchronize(st), "sync u0")) { rc = TILD_ERR_CUDA; break; }
-    c->styles_k[s].uk0 = (float)u0;
+    hd.suk0[s] = (float)u0;
     // real-space force table f_beta(r), unnormalised inverse transform
     for (int beta = 0; beta < D && rc == TILD_OK; beta++) {
       k_force_kernel<<<nblk(g.Mh, 256), 256, 0, st>>>(zbuf, ufull, g, D, beta);
@@ -285,23 +287,25 @@ int tild_build_tables(tild_ctx* c) {
     // CalcVirial applies to rho_k (pair_style.cu:277-279), stored on the half spectrum.
     const int ab[6][2] = {{0, 0}, {1, 1}, {2, 2}, {1, 0}, {2, 0}, {2, 1}};   // (alpha, beta)
     const int ab2[3][2] = {{0, 0}, {1, 1}, {1, 0}};
-    for (int j = 0; j < c->nP && rc == TILD_OK; j++) {
+    for (int j = 0; j < h.nP && rc == TILD_OK; j++) {
       const int alpha = (D == 3) ? ab[j][0] : ab2[j][0];
       const int beta = (D == 3) ? ab[j][1] : ab2[j][1];
       k_virial_real<<<nblk(g.M, 256), 256, 0, st>>>(vr, freal + (long long)beta * Mpad, g, D, alpha);
       c->launches++;
       if (tild_check_fft(c, cufftExecD2Z(pd2z, vr, zbuf2), "exec d2z")) { rc = TILD_ERR_CUDA; break; }
-      k_store_virk<<<nblk(g.Mh, 256), 256, 0, st>>>(c->virk + ((long long)s * c->nP + j) * g.Mh, zbuf2, g.Mh, invM * invM);
+      k_store_virk<<<nblk(g.Mh, 256), 256, 0, st>>>(c->virk + h.virk0 + ((long long)s * h.nP + j) * g.Mh, zbuf2, g.Mh,
+                                                    invM * invM);
       c->launches++;
     }
   }
-  if (rc == TILD_OK && c->C) {
-    k_charge_table<<<nblk(g.Mh, 256), 256, 0, st>>>(c->ctab, g, D, c->cfg.bjerrum, c->cfg.smearing, ref, invM);
+  if (rc == TILD_OK && h.C) {
+    k_charge_table<<<nblk(g.Mh, 256), 256, 0, st>>>(c->ctab + h.ctab0, g, D, h.cfg.bjerrum, h.cfg.smearing, ref, invM);
     c->launches++;
   }
-  for (size_t f = 0; f < c->fields.size() && rc == TILD_OK; f++) {
-    const tild_pair_style& ps = c->cfg.styles[c->fields[f].slot];
-    k_fieldphase<<<nblk(g.M, 256), 256, 0, st>>>(c->frfield + (long long)f * D * g.M, g, D, ps.prefactor, ps.phase, ps.dir,
+  for (const FieldK& fk : c->fields) {
+    if (fk.sys != si || rc != TILD_OK) continue;
+    const tild_pair_style& ps = h.cfg.styles[fk.cfg_index];
+    k_fieldphase<<<nblk(g.M, 256), 256, 0, st>>>(c->frfield + fk.fr0, g, D, ps.prefactor, ps.phase, ps.dir,
                                                  ps.n_periods, ref);
     c->launches++;
   }
@@ -314,14 +318,4 @@ int tild_build_tables(tild_ctx* c) {
   cudaFree(freal);
   cudaFree(vr);
   return rc;
-}
-
-double tild_ramp_ratio(const tild_ctx* c, int s, int64_t step) {
-  // PairStyle::Update (pair_style.cu:347-367) rescales the tables after every step so that
-  // u_k(0) equals A_i + (A_i - A_f) * (step + 1) / max_steps; forces of step n >= 2 see the
-  // update made at the end of step n - 1.
-  const StyleK& k = c->styles_k[s];
-  if (!k.ramp || step < 2 || c->max_steps <= 0) return 1.0;
-  const double target = (double)k.Ai + ((double)k.Ai - (double)k.Af) * (double)step / (double)c->max_steps;
-  return target / (double)k.uk0;
 }

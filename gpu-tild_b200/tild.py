@@ -99,6 +99,15 @@ def lib() -> C.CDLL:
         "tild_profile_steps": ([vp, i32, dp, i32, ip, C.c_char_p, i32], i32),
         "tild_time_steps": ([vp, i32, dp], i32), "tild_kernel_launches": ([vp, i64p], i32),
         "tild_sync": ([vp], i32),
+        "tild_batch_create": ([C.POINTER(Config), i32, i32, C.POINTER(vp)], i32), "tild_batch_destroy": ([vp], i32),
+        "tild_batch_last_error": ([vp], C.c_char_p),
+        "tild_batch_set_topology": ([vp, i32, ip, fp, ip, ip, ip], i32),
+        "tild_batch_set_state": ([vp, i32, fp, fp, fp], i32), "tild_batch_get_state": ([vp, i32, fp, fp, fp], i32),
+        "tild_batch_set_active": ([vp, i32, i32], i32), "tild_batch_set_step": ([vp, i32, C.c_int64], i32),
+        "tild_batch_get_step": ([vp, i32, i64p], i32), "tild_batch_step": ([vp, i32], i32),
+        "tild_batch_forces": ([vp, i32, fp], i32), "tild_batch_observables": ([vp, i32, C.POINTER(Obs)], i32),
+        "tild_batch_get_density": ([vp, i32, fp], i32), "tild_batch_time_steps": ([vp, i32, dp], i32),
+        "tild_batch_sync": ([vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -352,3 +361,111 @@ class Context:
 
     def sync(self):
         self._check(lib().tild_sync(self._h), "tild_sync")
+
+
+class Batch:
+    """Many independent systems advanced together (a tild_batch): one launch per stage for all
+    systems, one batched cuFFT plan per grid shape.  Systems share dim, pmeorder and rng."""
+
+    def __init__(self, systems: Sequence[System], device: int = 0):
+        L = lib()
+        self.systems = list(systems)
+        n = len(self.systems)
+        self._cfgs = (Config * n)(*[s.config() for s in self.systems])
+        h = C.c_void_p()
+        st = L.tild_batch_create(self._cfgs, n, device, C.byref(h))
+        if st != OK:
+            raise TildError(st, f"tild_batch_create failed: {L.tild_status_string(st).decode()}")
+        self._h = h
+        self._keep = []
+        for i, s in enumerate(self.systems):
+            self.set_topology(i, s)
+            self.set_state(i, s.x)
+
+    def _check(self, st: int, what: str):
+        if st != OK:
+            L = lib()
+            raise TildError(st, f"{what}: {L.tild_status_string(st).decode()}: {L.tild_batch_last_error(self._h).decode()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tild_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_topology(self, i: int, s: System):
+        types = np.ascontiguousarray(s.types, dtype=np.int32)
+        q = None if s.charges is None else np.ascontiguousarray(s.charges, dtype=np.float32)
+        nb = np.ascontiguousarray(s.n_bonds, dtype=np.int32)
+        bt = np.ascontiguousarray(s.bonded_to, dtype=np.int32).reshape(-1)
+        by = np.ascontiguousarray(s.bond_type, dtype=np.int32).reshape(-1)
+        self._check(lib().tild_batch_set_topology(self._h, i, _ptr(types, C.c_int32), _ptr(q, C.c_float),
+                                                  _ptr(nb, C.c_int32), _ptr(bt, C.c_int32), _ptr(by, C.c_int32)),
+                    "tild_batch_set_topology")
+
+    def set_state(self, i: int, x, xo=None, noise=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        xo = None if xo is None else np.ascontiguousarray(xo, dtype=np.float32)
+        noise = None if noise is None else np.ascontiguousarray(noise, dtype=np.float32)
+        self._check(lib().tild_batch_set_state(self._h, i, _ptr(x, C.c_float), _ptr(xo, C.c_float),
+                                               _ptr(noise, C.c_float)), "tild_batch_set_state")
+
+    def get_state(self, i: int):
+        s = self.systems[i]
+        x = np.empty((s.ns, s.dim), np.float32)
+        xo = np.empty_like(x)
+        nz = np.empty_like(x)
+        self._check(lib().tild_batch_get_state(self._h, i, _ptr(x, C.c_float), _ptr(xo, C.c_float),
+                                               _ptr(nz, C.c_float)), "tild_batch_get_state")
+        return x, xo, nz
+
+    def set_active(self, i: int, active: bool):
+        self._check(lib().tild_batch_set_active(self._h, i, 1 if active else 0), "tild_batch_set_active")
+
+    def set_step(self, i: int, step: int):
+        self._check(lib().tild_batch_set_step(self._h, i, int(step)), "tild_batch_set_step")
+
+    def step_count(self, i: int) -> int:
+        v = C.c_int64()
+        self._check(lib().tild_batch_get_step(self._h, i, C.byref(v)), "tild_batch_get_step")
+        return v.value
+
+    def step(self, n: int = 1):
+        self._check(lib().tild_batch_step(self._h, int(n)), "tild_batch_step")
+
+    def forces(self, i: int) -> np.ndarray:
+        s = self.systems[i]
+        f = np.empty((s.ns, s.dim), np.float32)
+        self._check(lib().tild_batch_forces(self._h, i, _ptr(f, C.c_float)), "tild_batch_forces")
+        return f
+
+    def observables(self, i: int) -> dict:
+        o = Obs()
+        self._check(lib().tild_batch_observables(self._h, i, C.byref(o)), "tild_batch_observables")
+        return o.as_dict()
+
+    def density(self, i: int) -> np.ndarray:
+        s = self.systems[i]
+        nch = s.ntypes + (1 if s.charges is not None else 0)
+        r = np.empty((nch, int(np.prod(s.nx[:s.dim]))), np.float32)
+        self._check(lib().tild_batch_get_density(self._h, i, _ptr(r, C.c_float)), "tild_batch_get_density")
+        return r
+
+    def time_steps(self, n: int) -> float:
+        ms = C.c_double()
+        self._check(lib().tild_batch_time_steps(self._h, int(n), C.byref(ms)), "tild_batch_time_steps")
+        return ms.value
+
+    def sync(self):
+        self._check(lib().tild_batch_sync(self._h), "tild_batch_sync")

@@ -221,6 +221,33 @@ int32_t tild_kernel_launches(tild_ctx* ctx, int64_t* count);
 /* Blocks until the context stream is idle; reports any device-side status flag. */
 int32_t tild_sync(tild_ctx* ctx);
 
+/* ---- batches: many independent systems advanced together ------------------------------------ */
+/* No single reference call corresponds: the reference runs one system per process.  A batch
+ * advances every system with one launch per stage (spread, k-space multiply, gather) and one
+ * batched cuFFT plan per grid shape.  Systems must share dim, pmeorder and rng; everything else
+ * (box, grid, types, styles, bonds, integrators, seed, time step) is per system.  Per-system
+ * calls take the system index `sys` (0..nsys-1) and mirror the single-system calls above. */
+typedef struct tild_batch tild_batch;
+int32_t tild_batch_create(const tild_config* cfgs, int32_t nsys, int32_t device, tild_batch** out);
+int32_t tild_batch_destroy(tild_batch* b);
+const char* tild_batch_last_error(const tild_batch* b);
+int32_t tild_batch_set_topology(tild_batch* b, int32_t sys, const int32_t* types, const float* charges,
+                                const int32_t* n_bonds, const int32_t* bonded_to, const int32_t* bond_type);
+int32_t tild_batch_set_state(tild_batch* b, int32_t sys, const float* x, const float* xo, const float* prev_noise);
+int32_t tild_batch_get_state(tild_batch* b, int32_t sys, float* x, float* xo, float* prev_noise);
+/* Systems marked inactive keep their state and are skipped by every per-step kernel. */
+int32_t tild_batch_set_active(tild_batch* b, int32_t sys, int32_t active);
+int32_t tild_batch_set_step(tild_batch* b, int32_t sys, int64_t step);
+int32_t tild_batch_get_step(tild_batch* b, int32_t sys, int64_t* step);
+/* nsteps steps of every active system. */
+int32_t tild_batch_step(tild_batch* b, int32_t nsteps);
+/* One force evaluation of every active system; forces of system `sys` to f if f != NULL. */
+int32_t tild_batch_forces(tild_batch* b, int32_t sys, float* f);
+int32_t tild_batch_observables(tild_batch* b, int32_t sys, tild_obs* out);
+int32_t tild_batch_get_density(tild_batch* b, int32_t sys, float* rho);
+int32_t tild_batch_time_steps(tild_batch* b, int32_t nsteps, double* ms);
+int32_t tild_batch_sync(tild_batch* b);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (code that
  * runs inside another framework's allocator, or after device allocation has been closed): the
