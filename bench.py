@@ -43,6 +43,56 @@ FALLBACK_HBM_GBS = 6650.0
 C_SIZEOF_OBS = __import__("ctypes").sizeof(tild.Obs)
 
 
+def ensemble(n: int = 256):
+    return [ts.ensemble_member(i) for i in range(n)]
+
+
+def run_ensemble(args):
+    """Batched ensemble: 256 independent diblock systems (box L ~ U(12, 24) snapped to dx = 0.5,
+    grids 24^3..48^3, N ~ U{10..40}, f_A ~ U(0.3, 0.7), chi N ~ U(10, 30), rho0 = 5) advanced
+    together, against the same systems run one at a time (a sample of them, scaled)."""
+    grp = tild_dist.Group(backend="nccl")
+    systems = ensemble(args.nsys)
+    mine = tild_dist.shard([s.ns for s in systems], grp.rank, grp.world)
+    local = [systems[i] for i in mine]
+    B = tild.Batch(local, device=grp.local)
+    B.step(args.warmup * 32)
+    B.sync()
+    grp.barrier()
+    with ClockSampler(grp.local) as clk:
+        ms = B.time_steps(args.steps)
+    ms = grp.max(ms)
+    tot = grp.sum(sum(s.ns for s in local)) * args.steps
+    value = tot / (ms / 1e3)
+    prof = B.profile_steps(args.steps)
+    B.close()
+    out = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": grp.world,
+           "steps": args.steps, "warmup": args.warmup * 32, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak" if grp.world == 1 else "strong", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded random-walk chains)",
+           "config": {"workload": f"ensemble_{args.nsys}_diblock_24^3-48^3_gaussian_p1_GJF",
+                      "systems": args.nsys, "beads_total": sum(s.ns for s in systems),
+                      "grid_points_total": int(sum(np.prod(s.nx) for s in systems)), "parallelism": f"shards{grp.world}"},
+           "clocks": clk.summary(), "stages_ms_per_step": {k: v / args.steps for k, v in prof.items()}}
+    if grp.rank == 0 and not args.no_serial:
+        # one at a time: every 16th system alone, scaled to all systems by their bead counts
+        sample = list(range(0, args.nsys, 16))
+        t_serial, ns_sample = 0.0, 0
+        for i in sample:
+            s = systems[i]
+            with tild.Context(s, device=grp.local) as c:
+                c.step(args.warmup * 32)
+                t_serial += c.time_steps(args.steps) / 1e3
+                ns_sample += s.ns
+        serial_value = ns_sample * args.steps / t_serial
+        out["serial"] = {"value": serial_value, "unit": "particle-steps/s",
+                         "sample": f"{len(sample)} of {args.nsys} systems, each alone for {args.steps} steps"}
+        out["batched_over_serial"] = value / serial_value
+    grp.close()
+    if grp.rank == 0:
+        print(json.dumps(out))
+
+
 def make_system(workload: str):
     if workload == "blend":
         return ts.homopolymer_blend(), "blend_2.6M_128^3_gaussian_erf_p3_GJF"
@@ -280,7 +330,9 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate"])
+    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate", "ensemble"])
+    ap.add_argument("--nsys", type=int, default=256)
+    ap.add_argument("--no-serial", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
     args = ap.parse_args()
@@ -288,6 +340,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_ours(args)
 

@@ -97,7 +97,12 @@ void free_all(tild_ctx* c) {
       cufftDestroy(b.r2c);
       cufftDestroy(b.c2r);
     }
+  for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+  c->graphs.clear();
   tild_sort_free(c);
+  for (cudaStream_t a : c->aux) cudaStreamDestroy(a);
+  for (cudaEvent_t e : c->ev_join) cudaEventDestroy(e);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -406,7 +411,38 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
   cudaMemcpyAsync(c->cta_spec, tspec.data(), tspec.size() * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(c->cta_grid, tgrid.data(), tgrid.size() * 4, cudaMemcpyHostToDevice, st);
   if (tild_check(c, cudaStreamSynchronize(st), "init")) return TILD_ERR_CUDA;
-  // batched cuFFT plans, one pair per grid shape
+  // batched cuFFT plans, one pair per grid shape; with several shapes each plan runs on one of
+  // up to 8 auxiliary streams so transforms of different shapes overlap
+  if (c->buckets.size() > 1) {
+    const int naux = (int)std::min<size_t>(8, c->buckets.size());
+    c->aux.resize(naux);
+    c->ev_join.resize(naux);
+    for (int k = 0; k < naux; k++) {
+      if (tild_check(c, cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking), "aux stream") ||
+          tild_check(c, cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming), "aux event"))
+        return TILD_ERR_CUDA;
+    }
+    if (tild_check(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "fork event")) return TILD_ERR_CUDA;
+    // largest buckets first, each to the least loaded stream
+    std::vector<int> order(c->buckets.size());
+    for (size_t k = 0; k < order.size(); k++) order[k] = (int)k;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+      const Bucket& A = c->buckets[a];
+      const Bucket& B = c->buckets[b];
+      return (long long)A.nx[0] * A.nx[1] * A.nx[2] * A.channels > (long long)B.nx[0] * B.nx[1] * B.nx[2] * B.channels;
+    });
+    std::vector<long long> load(naux, 0);
+    for (int bi : order) {
+      int best = 0;
+      for (int k = 1; k < naux; k++)
+        if (load[k] < load[best]) best = k;
+      Bucket& b = c->buckets[bi];
+      b.lane = best;
+      load[best] += (long long)b.nx[0] * b.nx[1] * b.nx[2] * b.channels;
+    }
+  } else {
+    c->buckets[0].lane = -1;
+  }
   for (Bucket& b : c->buckets) {
     int n[3];
     if (c->D == 3) { n[0] = b.nx[2]; n[1] = b.nx[1]; n[2] = b.nx[0]; }
@@ -418,7 +454,8 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
       return TILD_ERR_CUDA;
     }
     b.planned = true;
-    if (tild_check_fft(c, cufftSetStream(b.r2c, st), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, st), "plan stream"))
+    cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : st;
+    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, bs), "plan stream"))
       return TILD_ERR_CUDA;
   }
   for (int s = 0; s < nsys && !rc; s++) rc = tild_build_tables(c, s);
@@ -549,13 +586,89 @@ bool all_ready(tild_ctx* c) {
   return true;
 }
 
+// Host bookkeeping of `n` integrating steps that ran inside a graph replay (the device side,
+// including step counters and buffer rotations, is in the graph).
+void account_replayed_steps(tild_ctx* c, int n, long long launches_per_step) {
+  for (int s = 0; s < c->nsys; s++) {
+    SysHost& h = c->sys[s];
+    if (!h.active) continue;
+    h.step += n;
+    c->h_sys[s].step = h.step;
+    h.forces_step = h.step;
+    h.have_forces = true;
+  }
+  c->launches += launches_per_step * n;
+  if (c->sort_interval > 0) c->sorts += n / c->sort_interval;
+}
+
+// n integrating steps.  Whole periods of graph_len steps (two sort periods, so every buffer
+// rotation and sort swap returns to its starting configuration) run as one CUDA graph, captured
+// once per buffer configuration and replayed afterwards; the rest run as direct launches.
+int run_steps(tild_ctx* c, int n) {
+  const int len = c->sort_interval > 0 ? 2 * c->sort_interval : c->graph_len;
+  while (n > 0) {
+    const bool aligned = c->sort_interval <= 0 || c->steps_since_sort >= c->sort_interval;
+    if (c->use_graphs && n >= len && aligned && !c->profiling) {
+      c->steps_since_sort = c->sort_interval;  // the graph always starts with a sort
+      const void* p0 = c->pos[0];
+      const int cur = c->cur;
+      cudaGraphExec_t exec = nullptr;
+      for (auto& ge : c->graphs)
+        if (ge.p0 == p0 && ge.cur == cur) exec = ge.exec;
+      if (!exec) {
+        const long long l0 = c->launches;
+        const int64_t step_before = c->sys[0].step;
+        std::vector<SysHost> saved_hosts;  // host counters advance during capture; restore, then replay
+        for (const SysHost& h : c->sys) saved_hosts.push_back(h);
+        const auto saved_hsys = c->h_sys;
+        const long long saved_sorts = c->sorts;
+        if (tild_check(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture"))
+          return TILD_ERR_CUDA;
+        int rc = TILD_OK;
+        for (int k = 0; k < len && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (rc) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        if (tild_check(c, e, "end capture")) return TILD_ERR_CUDA;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (tild_check(c, ei, "instantiate graph")) return TILD_ERR_CUDA;
+        (void)step_before;
+        // capture advanced the host mirrors without running anything: restore them
+        const long long per_step = (c->launches - l0) / len;
+        for (int s = 0; s < c->nsys; s++) {
+          c->sys[s].step = saved_hosts[s].step;
+          c->sys[s].forces_step = saved_hosts[s].forces_step;
+          c->sys[s].have_forces = saved_hosts[s].have_forces;
+        }
+        c->h_sys = saved_hsys;
+        c->sorts = saved_sorts;
+        c->launches = l0;
+        c->graphs.push_back({exec, p0, cur});
+        c->graph_launches_per_step = per_step;
+        // after capture the buffer configuration is back at (p0, cur): same as a replay
+      }
+      if (tild_check(c, cudaGraphLaunch(exec, c->stream), "graph launch")) return TILD_ERR_CUDA;
+      account_replayed_steps(c, len, c->graph_launches_per_step);
+      c->steps_since_sort = c->sort_interval;
+      n -= len;
+    } else {
+      int rc = tild_run_forces(c, true, nullptr, -1);
+      if (rc) return rc;
+      n -= 1;
+    }
+  }
+  return TILD_OK;
+}
+
 int engine_step(tild_ctx* c, int nsteps) {
   if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "every active system needs tild_set_state before stepping");
   cudaSetDevice(c->device);
-  for (int k = 0; k < nsteps; k++) {
-    int rc = tild_run_forces(c, true, nullptr, -1);
-    if (rc) return rc;
-  }
+  int rc = run_steps(c, nsteps);
+  if (rc) return rc;
   return tild_poll_status(c);
 }
 
@@ -616,8 +729,7 @@ int engine_time(tild_ctx* c, int nsteps, double* ms) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, c->stream);
-  int rc = TILD_OK;
-  for (int k = 0; k < nsteps && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
+  int rc = run_steps(c, nsteps);
   cudaEventRecord(e1, c->stream);
   cudaEventSynchronize(e1);
   float t = 0.f;

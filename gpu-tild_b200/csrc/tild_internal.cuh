@@ -104,11 +104,16 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
   int channels = 0;
   cufftHandle r2c = 0, c2r = 0;
   bool planned = false;
+  int lane = 0;                          // auxiliary stream index (-1: main stream)
 };
 
 struct tild_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // auxiliary streams: the FFTs of different grid shapes run concurrently (fork/join by events)
+  std::vector<cudaStream_t> aux;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   int D = 3, P = 1;
   int nsys = 1;
   std::vector<SysHost> sys;
@@ -183,6 +188,17 @@ struct tild_ctx {
   int64_t steps_since_sort = 0;
   long long sorts = 0;
   int spread_cap = 0;                    // shared-memory 32-bit words of the tiled spread
+
+  // CUDA graphs of whole step periods (tild_api.cu): keyed by the buffer configuration
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    const void* p0;
+    int cur;
+  };
+  std::vector<GraphEntry> graphs;
+  bool use_graphs = true;
+  int graph_len = 32;                    // graph length when the sort is disabled
+  long long graph_launches_per_step = 0;
 
   // per-stage timing (tild_profile_steps)
   std::vector<cudaEvent_t> prof_ev;

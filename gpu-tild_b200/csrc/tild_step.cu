@@ -136,7 +136,9 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   const long long M = g.M;
   const float ig = 1.0f / g.gvol;
   const bool qc = C && q != 0.f;
-  if (vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
+  // Order <= 1 stencils (8 nodes) spread straight into the global accumulator: for them zeroing
+  // and flushing a shared box costs more than the shared atomics save.
+  if (P >= 2 && vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
     const int tot = (int)vol * nch;
     for (int k = threadIdx.x; k < tot; k += blockDim.x) smi[k] = 0;
     __syncthreads();
@@ -252,11 +254,24 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
                                              int integrate) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
+  // per-CTA style table: the CTA covers one system
+  __shared__ float s_scale[TILD_MAX_STYLES];
+  __shared__ int s_ab[TILD_MAX_STYLES];
+  __shared__ int s_nfft;
+  const long long est = sd.step + (integrate ? 1 : 0);
+  if (threadIdx.x < TILD_MAX_STYLES && threadIdx.x < sd.nfft) {
+    s_scale[threadIdx.x] = ramp_ratio(sd, threadIdx.x, est);
+    s_ab[threadIdx.x] = sd.sa[threadIdx.x] | (sd.sb[threadIdx.x] << 8);
+  }
+  if (threadIdx.x == 0) s_nfft = sd.nfft;
+  __syncthreads();
   const Geom& g = sd.g;
   const long long h = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
   const long long Mh = g.Mh;
   if (h >= Mh) return;
   const int T = sd.T, C = sd.C;
+  const int nfft = s_nfft;
+  const float* utab = utab_all + sd.utab0 + h;
   const float2* rhok = rhok_all + sd.spec0;
   float2* gk = gk_all + sd.spec0 * D;
   const float* kd = kd_all + sd.kd0;
@@ -268,7 +283,6 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   kv[0] = kd[ix];
   kv[1] = kd[g.nx[0] + iy];
   kv[2] = (D == 3) ? kd[g.nx[0] + g.nx[1] + iz] : 0.f;
-  const long long est = sd.step + (integrate ? 1 : 0);
   if (NT > 0) {
     constexpr int NA = NT > 0 ? NT : 1;
     float2 rk[NA], phi[NA];
@@ -277,9 +291,9 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
       rk[t] = (t < T) ? rhok[(long long)t * Mh + h] : make_float2(0.f, 0.f);
       phi[t] = make_float2(0.f, 0.f);
     }
-    for (int k = 0; k < sd.nfft; k++) {
-      const float u = utab_all[sd.utab0 + (long long)k * Mh + h] * ramp_ratio(sd, k, est);
-      const int a = sd.sa[k], b = sd.sb[k];
+    for (int k = 0; k < nfft; k++) {
+      const float u = utab[(long long)k * Mh] * s_scale[k];
+      const int a = s_ab[k] & 0xff, b = s_ab[k] >> 8;
       // explicit selects keep rk[] and phi[] in registers
       float2 ra = make_float2(0.f, 0.f), rb = make_float2(0.f, 0.f);
 #pragma unroll
@@ -303,9 +317,9 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   } else {  // more types than the specialised kernels cover: same arithmetic, local arrays
     float2 phi[TILD_MAX_TYPES];
     for (int t = 0; t < T; t++) phi[t] = make_float2(0.f, 0.f);
-    for (int k = 0; k < sd.nfft; k++) {
-      const float u = utab_all[sd.utab0 + (long long)k * Mh + h] * ramp_ratio(sd, k, est);
-      const int a = sd.sa[k], b = sd.sb[k];
+    for (int k = 0; k < nfft; k++) {
+      const float u = utab[(long long)k * Mh] * s_scale[k];
+      const int a = s_ab[k] & 0xff, b = s_ab[k] >> 8;
       const float2 ra = rhok[(long long)a * Mh + h], rb = rhok[(long long)b * Mh + h];
       phi[a].x += u * rb.x; phi[a].y += u * rb.y;
       phi[b].x += u * ra.x; phi[b].y += u * ra.y;
@@ -388,7 +402,7 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ F, const floa
 }
 
 template <int D, int P, bool INTEG, bool XW>
-__global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather(
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather(
     const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
@@ -537,7 +551,11 @@ __global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
 template <int D, int P>
 void launch_spread(tild_ctx* c) {
   const size_t smem = sizeof(int) * (size_t)c->spread_cap;
-  cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
+  if (!(attr_devices >> (c->device & 63) & 1ull)) {
+    cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_devices |= 1ull << (c->device & 63);
+  }
   k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
                                                                    c->rho_fx, c->spread_cap, c->d_status);
 }
@@ -597,6 +615,23 @@ void launch_kmul(tild_ctx* c, bool integ) {
   }
 }
 
+// fork the auxiliary streams off the main stream, and join them back
+int fork(tild_ctx* c) {
+  if (c->aux.empty()) return 0;
+  if (tild_check(c, cudaEventRecord(c->ev_fork, c->stream), "fork")) return 1;
+  for (cudaStream_t a : c->aux)
+    if (tild_check(c, cudaStreamWaitEvent(a, c->ev_fork, 0), "fork wait")) return 1;
+  return 0;
+}
+
+int join(tild_ctx* c) {
+  for (size_t k = 0; k < c->aux.size(); k++) {
+    if (tild_check(c, cudaEventRecord(c->ev_join[k], c->aux[k]), "join")) return 1;
+    if (tild_check(c, cudaStreamWaitEvent(c->stream, c->ev_join[k], 0), "join wait")) return 1;
+  }
+  return 0;
+}
+
 }  // namespace
 
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
@@ -613,17 +648,21 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   c->launches += 2;
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
+  if (fork(c)) return TILD_ERR_CUDA;
   for (auto& b : c->buckets)
     if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+  if (join(c)) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_KMUL);
   if (c->D == 3) launch_kmul<3>(c, integrate);
   else launch_kmul<2>(c, integrate);
   c->launches++;
   if (tild_check(c, cudaGetLastError(), "kmul")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_C2R);
+  if (fork(c)) return TILD_ERR_CUDA;
   for (auto& b : c->buckets)
     if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
       return TILD_ERR_CUDA;
+  if (join(c)) return TILD_ERR_CUDA;
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
   for (const FieldK& fk : c->fields) {
     const SysHost& h = c->sys[fk.sys];
@@ -643,7 +682,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   c->launches++;
   if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
   if (integrate) {
-    bool any_inactive = false;
+    bool any_inactive = c->nsys > 1;  // batches always carry the hold kernel (graphs stay valid)
     for (const SysHost& h : c->sys) any_inactive |= !h.active;
     if (any_inactive) {
       k_hold_inactive<<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->pos[c->cur ^ 1], c->cta_bead,

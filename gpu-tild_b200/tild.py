@@ -467,5 +467,13 @@ class Batch:
         self._check(lib().tild_batch_time_steps(self._h, int(n), C.byref(ms)), "tild_batch_time_steps")
         return ms.value
 
+    def profile_steps(self, n: int) -> dict:
+        """Per-stage CUDA-event times over n steps (a batch is a context of several systems)."""
+        out = (C.c_double * 16)()
+        cnt = C.c_int32()
+        names = C.create_string_buffer(512)
+        self._check(lib().tild_profile_steps(self._h, int(n), out, 16, C.byref(cnt), names, 512), "tild_profile_steps")
+        return {k: out[i] for i, k in enumerate(names.value.decode().split(","))}
+
     def sync(self):
         self._check(lib().tild_batch_sync(self._h), "tild_batch_sync")
