@@ -107,23 +107,46 @@ def make_system(workload: str):
 # algorithmic bytes per launch of each stage (the roofline numerators)
 # ------------------------------------------------------------------------------------------
 def stage_bytes(s) -> dict:
+    """Compulsory HBM bytes of one launch of each stage's kernel, each array touched once."""
     ns, D, T = s.ns, s.dim, s.ntypes
     C = 1 if s.charges is not None else 0
     M = int(np.prod(s.nx[:D]))
     Mh = M // s.nx[0] * (s.nx[0] // 2 + 1)
     nfft = sum(1 for st in s.styles if st.kind != tild.STYLE_FIELDPHASE)
     gjf = any(k == tild.INTEGRATOR_GJF for k, _ in s.integrators)
-    per_bead_gather = 16 + 4 + 12 + 16 + 16 + (24 if gjf else 0) + (4 if C else 0)
+    # x_n (16), bead id, bond info, partners (4 + 4 + 12), x_{n-1} read and x_{n+1} write (32),
+    # GJF noise read and write (24), charge (4)
+    per_bead_gather = 16 + 20 + 32 + (24 if gjf else 0) + 4 * C
     return {
         "sort": 0,
-        "fix2float": (T + C) * M * (8 + 8 + 4),
-        "spread": ns * (16 + (4 if C else 0)) + (T + C) * M * 4,
+        "fix2float": (T + C) * M * (8 + 4 + 8),            # read u64, write f32, clear u64
+        "spread": ns * (16 + 4 * C) + (T + C) * M * 16,     # positions; u64 accumulator RMW
         "r2c": (T + C) * (M * 4 + Mh * 8),
-        "kmul": (T + C) * Mh * 8 + nfft * Mh * 4 + (C * Mh * 4) + (T + C) * D * Mh * 8,
+        "kmul": (T + C) * Mh * 8 + nfft * Mh * 4 + C * Mh * 4 + (T + C) * D * Mh * 8,
         "c2r": (T + C) * D * (Mh * 8 + M * 4),
         "fieldphase": 0,
-        "gather": ns * per_bead_gather + (T + C) * D * M * 4,
+        "interleave": (T + C) * M * (D * 4 + 16),
+        "gather": ns * per_bead_gather + (T + C) * M * 16,  # every float4 field node read once
+        "step_tail": 0,
     }
+
+
+def step_bytes(s) -> int:
+    """Compulsory bytes of one whole step of a fused design: ns * b_p + M * 48 * channels, with
+    b_p = 104 B per bead for GJF (64 for EM, +4 with charges)."""
+    D = s.dim
+    M = int(np.prod(s.nx[:D]))
+    C = 1 if s.charges is not None else 0
+    gjf = any(k == tild.INTEGRATOR_GJF for k, _ in s.integrators)
+    bp = (104 if gjf else 64) + 4 * C
+    return s.ns * bp + M * 48 * (s.ntypes + C)
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the stage's kernel, from one ncu
+# capture of that kernel on the same workload (summaries and commands under profiles/)
+NCU_DRAM_BYTES_PER_LAUNCH = {
+    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 290827776, "spread": 75483392},
+}
 
 
 def hbm_peak():
@@ -249,7 +272,11 @@ def run_ours(args):
         "stages_ms_per_step": {k: v / args.steps for k, v in prof.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": f"{peak_kind} ({'MEASURED_PEAKS.json' if peak_kind == 'measured' else 'fallback'})",
-                     "algorithmic_bytes_per_launch": sb[dom], "traffic": None},
+                     "algorithmic_bytes_per_launch": sb[dom],
+                     "traffic": NCU_DRAM_BYTES_PER_LAUNCH.get(wname, {}).get(dom)},
+        "step_roofline": {"algorithmic_bytes_per_step": step_bytes(s),
+                          "achieved": step_bytes(s) * args.steps / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": step_bytes(s) * args.steps / (ms / 1e3) / 1e9 / peak},
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(s, args)

@@ -209,8 +209,11 @@ struct tild_ctx {
   std::string err;
 };
 
-enum TildStage { STAGE_SORT = 0, STAGE_ZERO, STAGE_SPREAD, STAGE_R2C, STAGE_KMUL, STAGE_C2R, STAGE_FIELD, STAGE_GATHER, STAGE_COUNT };
-static const char* const kStageNames[STAGE_COUNT] = {"sort", "fix2float", "spread", "r2c", "kmul", "c2r", "fieldphase", "gather"};
+enum TildStage {
+  STAGE_SORT = 0, STAGE_ZERO, STAGE_SPREAD, STAGE_R2C, STAGE_KMUL, STAGE_C2R, STAGE_FIELD, STAGE_INTERLEAVE, STAGE_GATHER,
+  STAGE_TAIL, STAGE_COUNT
+};
+static const char* const kStageNames[STAGE_COUNT] = {"sort", "fix2float", "spread", "r2c", "kmul", "c2r", "fieldphase", "interleave", "gather", "step_tail"};
 
 // Records the start of a stage when profiling (the next mark, or the final one, ends it).
 inline void tild_mark(tild_ctx* c, int stage) {

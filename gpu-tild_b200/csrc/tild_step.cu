@@ -670,18 +670,20 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
                                                                  c->frfield + fk.fr0, fk.a, fk.b, c->D, h.g.M);
     c->launches++;
   }
-  tild_mark(c, STAGE_GATHER);
+  tild_mark(c, STAGE_INTERLEAVE);
   {
     int* blk0 = c->cta_grid + c->n_cta_grid;
     if (c->D == 3) k_interleave<3><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
     else k_interleave<2><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
     c->launches++;
   }
+  tild_mark(c, STAGE_GATHER);
   if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys);
   else dispatch_p_gather<2>(c, integrate, f_bead, f_sys);
   c->launches++;
   if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
   if (integrate) {
+    tild_mark(c, STAGE_TAIL);
     bool any_inactive = c->nsys > 1;  // batches always carry the hold kernel (graphs stay valid)
     for (const SysHost& h : c->sys) any_inactive |= !h.active;
     if (any_inactive) {
