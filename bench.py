@@ -93,6 +93,64 @@ def run_ensemble(args):
         print(json.dumps(out))
 
 
+def run_serving(args):
+    """Serving: a seeded Poisson stream (mean --rate jobs/s) of jobs drawn from the batched-ensemble
+    distribution, each --job-steps steps returning its energy trace and avg_sk, served by
+    continuous batching over a slot pool (--slots-per-edge slots for each grid edge 24..48).
+    value: aggregate particle-steps/s of all jobs over the span from the first arrival to the
+    last completion; latency percentiles are arrival -> results on the host.  Against: the same
+    jobs run one at a time alone (a sample of them, each for all its steps)."""
+    import tild_serve as sv
+    grp = tild_dist.Group(backend="nccl")
+    jobs_all = sv.poisson_jobs(args.jobs, args.rate, steps=args.job_steps)
+    mine = [j for k, j in enumerate(jobs_all) if k % grp.world == grp.rank]
+    # each rank replays its share of the stream: arrivals keep their absolute times
+    edges = {g: args.slots_per_edge for g in ts.ensemble_grid_edges()}
+    with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch) as srv:
+        pool_bytes, nslots = srv.pool_bytes, srv.nslots
+        grp.barrier()
+        res = srv.run(mine, clock="wall")
+        stepping_s = srv.stepping_s
+    rows = grp.gather_lists([(r.job_id, r.ns, r.steps, r.arrival, r.admitted, r.finished) for r in res])
+    rows.sort()
+    results = [sv.JobResult(j, ns, 0, st, a, admitted=ad, finished=f) for j, ns, st, a, ad, f in rows]
+    summ = sv.latency_summary(results)
+    work = sum(r.ns * r.steps for r in results)
+    offered = args.rate * work / len(results)
+    out = {"metric": "particle-steps/s (aggregate, served jobs); p50/p99 job latency", "value":
+           summ["aggregate_particle_steps_per_s"], "unit": "particle-steps/s", "n_gpus": grp.world,
+           "steps": args.job_steps, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic (seeded random-walk chains, seeded Poisson arrivals)",
+           "config": {"workload": f"serving_poisson{args.rate:g}_{args.jobs}jobs_{args.job_steps}steps",
+                      "slots": nslots * grp.world, "slots_per_edge": args.slots_per_edge, "epoch_steps": args.epoch,
+                      "hbm_budget_gb": args.hbm_budget / 1e9, "pool_gb_per_gpu": pool_bytes / 1e9,
+                      "parallelism": f"replicas{grp.world}"},
+           "latency": summ,
+           "offered_particle_steps_per_s": offered,
+           "stepping_fraction_rank0": stepping_s / summ["span_s"] if summ["span_s"] > 0 else None}
+    if grp.rank == 0 and not args.no_serial:
+        sample = jobs_all[:: max(1, len(jobs_all) // args.serial_sample)][:args.serial_sample]
+        t_serial, w_serial, lat = 0.0, 0, []
+        for j in sample:
+            t0 = time.perf_counter()
+            with tild.Context(j.system, device=grp.local) as c:
+                c.step(j.steps)
+                c.observables()
+                c.sync()
+            dt = time.perf_counter() - t0
+            t_serial += dt
+            lat.append(dt)
+            w_serial += j.system.ns * j.steps
+        out["serial"] = {"value": w_serial / t_serial, "unit": "particle-steps/s",
+                         "job_time_s_mean": float(np.mean(lat)),
+                         "sample": f"{len(sample)} of {len(jobs_all)} jobs, each alone for all its steps "
+                                   "(set-up included)"}
+        out["served_over_serial"] = out["value"] / out["serial"]["value"]
+    grp.close()
+    if grp.rank == 0:
+        print(json.dumps(out))
+
+
 def make_system(workload: str):
     if workload == "blend":
         return ts.homopolymer_blend(), "blend_2.6M_128^3_gaussian_erf_p3_GJF"
@@ -357,8 +415,15 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate", "ensemble"])
+    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate", "ensemble", "serving"])
     ap.add_argument("--nsys", type=int, default=256)
+    ap.add_argument("--jobs", type=int, default=300, help="serving: number of jobs in the stream")
+    ap.add_argument("--rate", type=float, default=50.0, help="serving: mean arrivals per second")
+    ap.add_argument("--job-steps", type=int, default=5000)
+    ap.add_argument("--slots-per-edge", type=int, default=12)
+    ap.add_argument("--epoch", type=int, default=128)
+    ap.add_argument("--hbm-budget", type=float, default=80e9)
+    ap.add_argument("--serial-sample", type=int, default=6)
     ap.add_argument("--no-serial", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
@@ -369,6 +434,8 @@ def main():
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

@@ -92,6 +92,7 @@ void free_all(tild_ctx* c) {
   for (SysHost& h : c->sys)
     for (int i = 0; i < TILD_MAX_COMPUTES; i++)
       if (h.sk[i]) cudaFree(h.sk[i]);
+  tild_tables_free(c);
   for (Bucket& b : c->buckets)
     if (b.planned) {
       cufftDestroy(b.r2c);
@@ -180,7 +181,90 @@ int spread_kbits(int P, int D, double gvol, double qmax) {
   return k;
 }
 
-int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
+// Geometry of a system from its configuration (initialize.cu:30-60).
+void set_geometry(SysHost& h, const tild_config& cfg) {
+  h.D = cfg.dim;
+  h.T = cfg.ntypes;
+  h.C = cfg.do_charges ? 1 : 0;
+  h.ns = cfg.ns;
+  h.p = cfg.pmeorder;
+  h.nP = (h.D == 2) ? 3 : 6;
+  Geom& g = h.g;
+  g.M = 1;
+  h.S = 1;
+  float gv = 1.0f;
+  for (int d = 0; d < 3; d++) {
+    g.nx[d] = (d < h.D) ? cfg.nx[d] : 1;
+    g.L[d] = (d < h.D) ? cfg.box[d] : 1.0f;
+    g.Lh[d] = 0.5f * g.L[d];
+    g.dx[d] = g.L[d] / (float)g.nx[d];
+  }
+  h.dV = 1.0;
+  h.V = 1.0;
+  for (int d = 0; d < h.D; d++) {
+    gv *= g.dx[d];
+    g.M *= g.nx[d];
+    h.S *= (h.p + 1);
+    h.dV *= (double)g.dx[d];
+    h.V *= (double)g.L[d];
+  }
+  g.gvol = gv;
+  g.nxh = g.nx[0] / 2 + 1;
+  g.Mh = g.M / g.nx[0] * g.nxh;
+}
+
+// Physics part of system s's device descriptor (styles, integrators, masses, bonds) from h.cfg;
+// the layout part (slots, offsets) and the step counter are left as they are.
+void set_params(tild_ctx* c, int s) {
+  SysHost& h = c->sys[s];
+  const tild_config& cfg = h.cfg;
+  SysDev& d = c->h_sys[s];
+  h.fft_cfg.clear();
+  int nfft = 0;
+  for (int i = 0; i < cfg.n_styles; i++) {
+    const tild_pair_style& ps = cfg.styles[i];
+    if (ps.style == TILD_STYLE_FIELDPHASE) continue;
+    d.sa[nfft] = ps.type1;
+    d.sb[nfft] = ps.type2;
+    d.sramp[nfft] = ps.ramp;
+    d.sAi[nfft] = ps.prefactor;
+    d.sAf[nfft] = ps.final_prefactor;
+    d.suk0[nfft] = 1.0f;
+    h.fft_cfg.push_back(i);
+    nfft++;
+  }
+  for (int t = 0; t < TILD_MAX_TYPES; t++) h.type_integ_mask[t] = 0;
+  for (int t = 0; t < h.T; t++) {
+    int m = 0;
+    for (int k = 0; k < cfg.n_integrators; k++)
+      if (cfg.integrators[k].group_type < 0 || cfg.integrators[k].group_type == t) m |= 1 << k;
+    h.type_integ_mask[t] = m;
+  }
+  d.g = h.g;
+  d.T = h.T;
+  d.C = h.C;
+  d.nfft = nfft;
+  d.ns = h.ns;
+  d.max_steps = cfg.max_steps;
+  d.seed = cfg.seed;
+  d.delt = cfg.delt;
+  d.noise_mag = cfg.noise_mag;
+  d.n_integ = cfg.n_integrators;
+  for (int k = 0; k < cfg.n_integrators; k++) d.integ_kind[k] = cfg.integrators[k].kind;
+  for (int t = 0; t < h.T; t++) {
+    d.type_mask[t] = h.type_integ_mask[t];
+    d.mass[t] = cfg.mass[t];
+    d.diff[t] = cfg.diff[t];
+  }
+  for (int b = 0; b < cfg.n_bond_types; b++) {
+    d.bond_k[b] = cfg.bond_k[b];
+    d.bond_req[b] = cfg.bond_req[b];
+  }
+  h.kbits = spread_kbits(h.p, h.D, h.g.gvol, 1.0);
+  d.kbits = h.kbits;
+}
+
+int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, const int32_t* capacity) {
   std::string why;
   for (int s = 0; s < nsys; s++) {
     int v = validate(&cfgs[s], why);
@@ -212,69 +296,27 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
     const tild_config& cfg = cfgs[s];
     SysHost& h = c->sys[s];
     h.cfg = cfg;
-    h.D = cfg.dim;
-    h.T = cfg.ntypes;
-    h.C = cfg.do_charges ? 1 : 0;
-    h.ns = cfg.ns;
-    h.p = cfg.pmeorder;
-    h.nP = (h.D == 2) ? 3 : 6;
-    Geom& g = h.g;
-    g.M = 1;
-    h.S = 1;
-    float gv = 1.0f;
-    for (int d = 0; d < 3; d++) {
-      g.nx[d] = (d < h.D) ? cfg.nx[d] : 1;
-      g.L[d] = (d < h.D) ? cfg.box[d] : 1.0f;
-      g.Lh[d] = 0.5f * g.L[d];
-      g.dx[d] = g.L[d] / (float)g.nx[d];
-    }
-    h.dV = 1.0;
-    h.V = 1.0;
-    for (int d = 0; d < h.D; d++) {
-      gv *= g.dx[d];
-      g.M *= g.nx[d];
-      h.S *= (h.p + 1);
-      h.dV *= (double)g.dx[d];
-      h.V *= (double)g.L[d];
-    }
-    g.gvol = gv;
-    g.nxh = g.nx[0] / 2 + 1;
-    g.Mh = g.M / g.nx[0] * g.nxh;
-    h.ns_pad = (h.ns + kTile - 1) / kTile * kTile;
+    set_geometry(h, cfg);
+    const Geom& g = h.g;
+    h.cap = capacity ? std::max(h.ns, (int)capacity[s]) : h.ns;
+    h.ns_pad = (h.cap + kTile - 1) / kTile * kTile;
     h.slot0 = (int)slots;
     h.bead0 = (int)beads;
     slots += h.ns_pad;
-    beads += h.ns;
-    SysDev& d = c->h_sys[s];
-    int nfft = 0;
-    for (int i = 0; i < cfg.n_styles; i++) {
-      const tild_pair_style& ps = cfg.styles[i];
-      if (ps.style == TILD_STYLE_FIELDPHASE) {
+    beads += h.cap;
+    for (int i = 0; i < cfg.n_styles; i++)
+      if (cfg.styles[i].style == TILD_STYLE_FIELDPHASE) {
         FieldK f;
         f.sys = s;
-        f.a = ps.type1;
-        f.b = ps.type2;
+        f.a = cfg.styles[i].type1;
+        f.b = cfg.styles[i].type2;
         f.cfg_index = i;
         f.fr0 = fr;
         fr += (long long)h.D * g.M;
         c->fields.push_back(f);
-      } else {
-        d.sa[nfft] = ps.type1;
-        d.sb[nfft] = ps.type2;
-        d.sramp[nfft] = ps.ramp;
-        d.sAi[nfft] = ps.prefactor;
-        d.sAf[nfft] = ps.final_prefactor;
-        d.suk0[nfft] = 1.0f;
-        h.fft_cfg.push_back(i);
-        nfft++;
       }
-    }
-    for (int t = 0; t < h.T; t++) {
-      int m = 0;
-      for (int k = 0; k < cfg.n_integrators; k++)
-        if (cfg.integrators[k].group_type < 0 || cfg.integrators[k].group_type == t) m |= 1 << k;
-      h.type_integ_mask[t] = m;
-    }
+    set_params(c, s);
+    const int nfft = (int)h.fft_cfg.size();
     h.utab0 = utab;
     utab += (long long)nfft * g.Mh;
     h.virk0 = virk;
@@ -296,13 +338,9 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
     }
     c->buckets[bi].systems.push_back(s);
     h.bucket = bi;
-    // device descriptor
-    d.g = g;
-    d.T = h.T;
-    d.C = h.C;
-    d.nfft = nfft;
+    // layout part of the device descriptor
+    SysDev& d = c->h_sys[s];
     d.slot0 = h.slot0;
-    d.ns = h.ns;
     d.ns_pad = h.ns_pad;
     d.bead0 = h.bead0;
     d.active = 1;
@@ -310,23 +348,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
     d.ctab0 = h.ctab0;
     d.kd0 = h.kd0;
     d.step = 0;
-    d.max_steps = cfg.max_steps;
-    d.seed = cfg.seed;
-    d.delt = cfg.delt;
-    d.noise_mag = cfg.noise_mag;
-    d.n_integ = cfg.n_integrators;
-    for (int k = 0; k < cfg.n_integrators; k++) d.integ_kind[k] = cfg.integrators[k].kind;
-    for (int t = 0; t < h.T; t++) {
-      d.type_mask[t] = h.type_integ_mask[t];
-      d.mass[t] = cfg.mass[t];
-      d.diff[t] = cfg.diff[t];
-    }
-    for (int b = 0; b < cfg.n_bond_types; b++) {
-      d.bond_k[b] = cfg.bond_k[b];
-      d.bond_req[b] = cfg.bond_req[b];
-    }
-    h.kbits = spread_kbits(h.p, h.D, g.gvol, 1.0);
-    d.kbits = h.kbits;
+    d.stop_at = -1;
   }
   // channel layout: bucket by bucket so each bucket is one batched transform
   long long grid = 0, spec = 0;
@@ -365,7 +387,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c) {
   tspec.insert(tspec.end(), bspec.begin(), bspec.end());
   tgrid.insert(tgrid.end(), bgrid.begin(), bgrid.end());
   int maxns = 1;
-  for (const SysHost& h : c->sys) maxns = std::max(maxns, h.ns);
+  for (const SysHost& h : c->sys) maxns = std::max(maxns, h.cap);
   const size_t NS = c->nslots;
   int rc = TILD_OK;
   rc = rc ? rc : dalloc(c, &c->pos[0], NS, "positions");
@@ -664,10 +686,30 @@ int run_steps(tild_ctx* c, int n) {
   return TILD_OK;
 }
 
+// Systems with a stop step leave the active set on the device (k_advance_steps): bring their
+// step counters and activity back into the host mirrors after every stepping call.
+int refresh_from_device(tild_ctx* c) {
+  if (!c->any_stop) return TILD_OK;
+  std::vector<SysDev> dev(c->nsys);
+  if (tild_check(c, cudaMemcpyAsync(dev.data(), c->d_sys, sizeof(SysDev) * c->nsys, cudaMemcpyDeviceToHost, c->stream),
+                 "download descriptors") ||
+      tild_check(c, cudaStreamSynchronize(c->stream), "sync descriptors"))
+    return TILD_ERR_CUDA;
+  for (int s = 0; s < c->nsys; s++) {
+    SysHost& h = c->sys[s];
+    h.step = dev[s].step;
+    c->h_sys[s].step = dev[s].step;
+    h.active = h.active && dev[s].active;
+    c->h_sys[s].active = h.active ? 1 : 0;
+  }
+  return TILD_OK;
+}
+
 int engine_step(tild_ctx* c, int nsteps) {
   if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "every active system needs tild_set_state before stepping");
   cudaSetDevice(c->device);
   int rc = run_steps(c, nsteps);
+  if (!rc) rc = refresh_from_device(c);
   if (rc) return rc;
   return tild_poll_status(c);
 }
@@ -737,7 +779,110 @@ int engine_time(tild_ctx* c, int nsteps, double* ms) {
   *ms = t;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (!rc) rc = refresh_from_device(c);
   return rc ? rc : tild_poll_status(c);
+}
+
+// Replaces the system of slot s by another of the same grid shape and channel layout.
+int sys_load(tild_ctx* c, int s, const tild_config* cfg) {
+  if (check_sys(c, s) || !cfg) return TILD_ERR_BAD_INPUT;
+  std::string why;
+  const int v = validate(cfg, why);
+  if (v) return set_err(c, v, why.c_str());
+  SysHost& h = c->sys[s];
+  if (cfg->dim != c->D || cfg->pmeorder != c->P || cfg->rng != c->rng)
+    return set_err(c, TILD_ERR_UNSUPPORTED, "dim, pmeorder and rng must match the batch");
+  for (int d = 0; d < 3; d++)
+    if ((d < c->D ? cfg->nx[d] : 1) != h.g.nx[d]) return set_err(c, TILD_ERR_UNSUPPORTED, "grid shape differs from the slot's");
+  if (cfg->ntypes != h.T || (cfg->do_charges ? 1 : 0) != h.C)
+    return set_err(c, TILD_ERR_UNSUPPORTED, "ntypes and do_charges must match the slot");
+  if (cfg->ns > h.cap) return set_err(c, TILD_ERR_UNSUPPORTED, "more beads than the slot holds");
+  int nfft = 0, nfield = 0, nfield_slot = 0;
+  for (int i = 0; i < cfg->n_styles; i++) (cfg->styles[i].style == TILD_STYLE_FIELDPHASE ? nfield : nfft)++;
+  for (const FieldK& fk : c->fields) nfield_slot += fk.sys == s;
+  if (nfft != (int)h.fft_cfg.size() || nfield != nfield_slot)
+    return set_err(c, TILD_ERR_UNSUPPORTED, "the slot's number of FFT pair styles and of fieldphases must match");
+  cudaSetDevice(c->device);
+  if (tild_check(c, cudaStreamSynchronize(c->stream), "sync before load")) return TILD_ERR_CUDA;
+  h.cfg = *cfg;
+  set_geometry(h, *cfg);
+  set_params(c, s);
+  bool fields_moved = false;
+  for (int i = 0, k = 0; i < cfg->n_styles; i++) {
+    if (cfg->styles[i].style != TILD_STYLE_FIELDPHASE) continue;
+    while (c->fields[k].sys != s) k++;
+    FieldK& fk = c->fields[k++];
+    fields_moved |= fk.a != cfg->styles[i].type1 || fk.b != cfg->styles[i].type2;
+    fk.a = cfg->styles[i].type1;
+    fk.b = cfg->styles[i].type2;
+    fk.cfg_index = i;
+  }
+  if (fields_moved) {  // the captured step graphs carry the fieldphase types as launch arguments
+    for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+    c->graphs.clear();
+  }
+  SysDev& d = c->h_sys[s];
+  d.step = 0;
+  d.stop_at = -1;
+  h.step = 0;
+  h.forces_step = 0;
+  h.active = false;
+  h.topo_set = h.state_set = h.have_forces = false;
+  for (int k = 0; k < TILD_MAX_COMPUTES; k++) {
+    if (h.sk[k] && tild_check(c, cudaMemsetAsync(h.sk[k], 0, sizeof(double2) * h.g.Mh, c->stream), "clear sk"))
+      return TILD_ERR_CUDA;
+    h.sk_calls[k] = 0;
+  }
+  const int rc = tild_build_tables(c, s);
+  if (rc) return rc;
+  return tild_upload_sys(c);
+}
+
+int sys_sk_accumulate(tild_ctx* c, int s, int slot, int type) {
+  if (check_sys(c, s) || slot < 0 || slot >= TILD_MAX_COMPUTES || type < 0 || type >= c->sys[s].T)
+    return TILD_ERR_BAD_INPUT;
+  if (!c->sys[s].have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
+  cudaSetDevice(c->device);
+  return tild_sk_acc_run(c, s, slot, type);
+}
+
+int sys_sk_get(tild_ctx* c, int s, int slot, double* sk, int32_t* ncalls) {
+  if (check_sys(c, s) || slot < 0 || slot >= TILD_MAX_COMPUTES) return TILD_ERR_BAD_INPUT;
+  cudaSetDevice(c->device);
+  const SysHost& h = c->sys[s];
+  const int n = h.sk[slot] ? h.sk_calls[slot] : 0;
+  if (ncalls) *ncalls = n;
+  if (!sk) return TILD_OK;
+  const Geom& g = h.g;
+  if (n == 0) {
+    memset(sk, 0, sizeof(double) * 2 * (size_t)g.M);
+    return TILD_OK;
+  }
+  std::vector<double> hb(2 * (size_t)g.Mh);
+  if (tild_check(c, cudaMemcpyAsync(hb.data(), h.sk[slot], sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, c->stream), "download sk") ||
+      tild_check(c, cudaStreamSynchronize(c->stream), "sync sk"))
+    return TILD_ERR_CUDA;
+  // expand the half spectrum: A(-k) = conj(A(k)) for A = rho_k * rho_k of a real density
+  const int N0 = g.nx[0], N1 = g.nx[1], N2 = g.nx[2];
+  for (int z = 0; z < N2; z++)
+    for (int y = 0; y < N1; y++)
+      for (int x = 0; x < N0; x++) {
+        const size_t id = (size_t)x + (size_t)N0 * (y + (size_t)N1 * z);
+        double re, im;
+        if (x < g.nxh) {
+          const size_t h2 = (size_t)x + (size_t)g.nxh * (y + (size_t)N1 * z);
+          re = hb[2 * h2];
+          im = hb[2 * h2 + 1];
+        } else {
+          const int xm = N0 - x, ym = (N1 - y) % N1, zm = (N2 - z) % N2;
+          const size_t h2 = (size_t)xm + (size_t)g.nxh * (ym + (size_t)N1 * zm);
+          re = hb[2 * h2];
+          im = -hb[2 * h2 + 1];
+        }
+        sk[2 * id] = re / n;
+        sk[2 * id + 1] = im / n;
+      }
+  return TILD_OK;
 }
 
 }  // namespace
@@ -801,11 +946,12 @@ const char* tild_status_string(int32_t s) {
 
 const char* tild_last_error(const tild_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-static int create_common(const tild_config* cfgs, int nsys, int device, tild_batch** out) {
+static int create_common(const tild_config* cfgs, int nsys, int device, tild_batch** out,
+                         const int32_t* capacity = nullptr) {
   if (!cfgs || !out || nsys < 1) return TILD_ERR_BAD_INPUT;
   *out = nullptr;
   tild_batch* c = new tild_batch();
-  const int rc = engine_create(cfgs, nsys, device, c);
+  const int rc = engine_create(cfgs, nsys, device, c, capacity);
   if (rc) {
     fprintf(stderr, "tild_create: %s\n", c->err.c_str());
     free_all(c);
@@ -883,51 +1029,9 @@ int32_t tild_get_stencil(tild_ctx* c, int32_t* inds, float* w) {
   return rc ? rc : tild_poll_status(c);
 }
 
-int32_t tild_sk_accumulate(tild_ctx* c, int32_t slot, int32_t type) {
-  if (!c || slot < 0 || slot >= TILD_MAX_COMPUTES || type < 0 || type >= c->sys[0].T) return TILD_ERR_BAD_INPUT;
-  if (!c->sys[0].have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
-  cudaSetDevice(c->device);
-  return tild_sk_acc_run(c, 0, slot, type);
-}
+int32_t tild_sk_accumulate(tild_ctx* c, int32_t slot, int32_t type) { return sys_sk_accumulate(c, 0, slot, type); }
 
-int32_t tild_sk_get(tild_ctx* c, int32_t slot, double* sk, int32_t* ncalls) {
-  if (!c || slot < 0 || slot >= TILD_MAX_COMPUTES) return TILD_ERR_BAD_INPUT;
-  cudaSetDevice(c->device);
-  const SysHost& h = c->sys[0];
-  const int n = h.sk[slot] ? h.sk_calls[slot] : 0;
-  if (ncalls) *ncalls = n;
-  if (!sk) return TILD_OK;
-  const Geom& g = h.g;
-  if (n == 0) {
-    memset(sk, 0, sizeof(double) * 2 * (size_t)g.M);
-    return TILD_OK;
-  }
-  std::vector<double> hb(2 * (size_t)g.Mh);
-  if (tild_check(c, cudaMemcpyAsync(hb.data(), h.sk[slot], sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, c->stream), "download sk") ||
-      tild_check(c, cudaStreamSynchronize(c->stream), "sync sk"))
-    return TILD_ERR_CUDA;
-  // expand the half spectrum: A(-k) = conj(A(k)) for A = rho_k * rho_k of a real density
-  const int N0 = g.nx[0], N1 = g.nx[1], N2 = g.nx[2];
-  for (int z = 0; z < N2; z++)
-    for (int y = 0; y < N1; y++)
-      for (int x = 0; x < N0; x++) {
-        const size_t id = (size_t)x + (size_t)N0 * (y + (size_t)N1 * z);
-        double re, im;
-        if (x < g.nxh) {
-          const size_t h2 = (size_t)x + (size_t)g.nxh * (y + (size_t)N1 * z);
-          re = hb[2 * h2];
-          im = hb[2 * h2 + 1];
-        } else {
-          const int xm = N0 - x, ym = (N1 - y) % N1, zm = (N2 - z) % N2;
-          const size_t h2 = (size_t)xm + (size_t)g.nxh * (ym + (size_t)N1 * zm);
-          re = hb[2 * h2];
-          im = -hb[2 * h2 + 1];
-        }
-        sk[2 * id] = re / n;
-        sk[2 * id + 1] = im / n;
-      }
-  return TILD_OK;
-}
+int32_t tild_sk_get(tild_ctx* c, int32_t slot, double* sk, int32_t* ncalls) { return sys_sk_get(c, 0, slot, sk, ncalls); }
 
 int32_t tild_nlist_build(tild_ctx* c, float rc, int32_t group_type, int32_t* cell_of, int32_t* neigh_count,
                          int32_t* neigh, int32_t* cell_max_out) {
@@ -1017,6 +1121,34 @@ int32_t tild_sync(tild_ctx* c) {
 int32_t tild_batch_create(const tild_config* cfgs, int32_t nsys, int32_t device, tild_batch** out) {
   return create_common(cfgs, nsys, device, out);
 }
+int32_t tild_batch_create_slots(const tild_config* cfgs, const int32_t* capacity, int32_t nsys, int32_t device,
+                                tild_batch** out) {
+  if (!capacity) return TILD_ERR_BAD_INPUT;
+  return create_common(cfgs, nsys, device, out, capacity);
+}
+int32_t tild_batch_load(tild_batch* b, int32_t sys, const tild_config* cfg) { return sys_load(b, sys, cfg); }
+int32_t tild_batch_capacity(tild_batch* b, int32_t sys, int32_t* capacity) {
+  if (check_sys(b, sys) || !capacity) return TILD_ERR_BAD_INPUT;
+  *capacity = b->sys[sys].cap;
+  return TILD_OK;
+}
+int32_t tild_batch_set_stop(tild_batch* b, int32_t sys, int64_t stop_at) {
+  if (check_sys(b, sys) || stop_at < -1) return TILD_ERR_BAD_INPUT;
+  b->h_sys[sys].stop_at = stop_at;
+  if (stop_at >= 0) b->any_stop = true;
+  return tild_upload_sys(b);
+}
+int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active) {
+  if (check_sys(b, sys) || !active) return TILD_ERR_BAD_INPUT;
+  *active = b->sys[sys].active ? 1 : 0;
+  return TILD_OK;
+}
+int32_t tild_batch_sk_accumulate(tild_batch* b, int32_t sys, int32_t slot, int32_t type) {
+  return sys_sk_accumulate(b, sys, slot, type);
+}
+int32_t tild_batch_sk_get(tild_batch* b, int32_t sys, int32_t slot, double* sk, int32_t* ncalls) {
+  return sys_sk_get(b, sys, slot, sk, ncalls);
+}
 int32_t tild_batch_destroy(tild_batch* b) { return tild_destroy(b); }
 const char* tild_batch_last_error(const tild_batch* b) { return tild_last_error(b); }
 int32_t tild_batch_set_topology(tild_batch* b, int32_t sys, const int32_t* types, const float* charges,
@@ -1031,6 +1163,8 @@ int32_t tild_batch_get_state(tild_batch* b, int32_t sys, float* x, float* xo, fl
 }
 int32_t tild_batch_set_active(tild_batch* b, int32_t sys, int32_t active) {
   if (check_sys(b, sys)) return TILD_ERR_BAD_INPUT;
+  if (active && b->h_sys[sys].stop_at >= 0 && b->sys[sys].step >= b->h_sys[sys].stop_at)
+    return set_err(b, TILD_ERR_STATE, "the system is at or past its stop step");
   b->sys[sys].active = active != 0;
   return tild_upload_sys(b);
 }

@@ -61,6 +61,7 @@ struct SysDev {
   long long spec0;                 // channel 0 in rhok (half-spectrum points)
   long long utab0, ctab0, kd0;     // offsets in utab, ctab, kd
   long long step;                  // completed steps (advanced on the device)
+  long long stop_at;               // the system turns inactive once step reaches it (-1: never)
   int max_steps;
   int sa[TILD_MAX_STYLES], sb[TILD_MAX_STYLES], sramp[TILD_MAX_STYLES];
   float sAi[TILD_MAX_STYLES], sAf[TILD_MAX_STYLES], suk0[TILD_MAX_STYLES];
@@ -86,6 +87,7 @@ struct SysHost {
   Geom g;
   double dV = 1.0, V = 1.0;
   int slot0 = 0, ns_pad = 0, bead0 = 0;  // bead0: first bead in the engine's bead numbering
+  int cap = 0;                           // beads the slot can hold (>= ns; tild_batch_load)
   long long grid0 = 0, spec0 = 0, utab0 = 0, ctab0 = 0, kd0 = 0, virk0 = 0;
   int kbits = 20;
   std::vector<int> fft_cfg;              // fft table slot -> config style index
@@ -204,6 +206,21 @@ struct tild_ctx {
   std::vector<cudaEvent_t> prof_ev;
   std::vector<int> prof_stage;
   bool profiling = false;
+
+  // FP64 table builds (tild_tables.cu): scratch sized for the largest grid, plans per grid shape
+  struct TablePlan {
+    int nx[3];
+    cufftHandle z2d, d2z;
+  };
+  std::vector<TablePlan> tab_plans;
+  long long tab_M = 0;
+  double* tab_ufull = nullptr;
+  cufftDoubleComplex* tab_z = nullptr;
+  cufftDoubleComplex* tab_z2 = nullptr;
+  double* tab_freal = nullptr;
+  double* tab_vr = nullptr;
+
+  bool any_stop = false;                 // some system has a device-side stop step
 
   long long launches = 0;
   std::string err;
@@ -337,6 +354,9 @@ int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
+int tild_table_scratch(tild_ctx* c);
+int tild_table_plans(tild_ctx* c, const Geom& g, int D, cufftHandle* z2d, cufftHandle* d2z);
+void tild_tables_free(tild_ctx* c);
 int tild_stencil_run(tild_ctx* c, int s, int* inds_dev, float* w_dev);
 int tild_nlist_geom(const SysHost& h, float rc, int* nc, float* Lc, int* total, int* cmax);
 int tild_nlist_run(tild_ctx* c, int s, float rc, int group_type, int* cell_of_bead_dev, int* ncount_dev,

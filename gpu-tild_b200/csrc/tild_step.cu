@@ -136,9 +136,7 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   const long long M = g.M;
   const float ig = 1.0f / g.gvol;
   const bool qc = C && q != 0.f;
-  // Order <= 1 stencils (8 nodes) spread straight into the global accumulator: for them zeroing
-  // and flushing a shared box costs more than the shared atomics save.
-  if (P >= 2 && vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
+  if (vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
     const int tot = (int)vol * nch;
     for (int k = threadIdx.x; k < tot; k += blockDim.x) smi[k] = 0;
     __syncthreads();
@@ -233,13 +231,72 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   }
 }
 
-// fixed-point grid -> FP32 density, clearing the accumulator for the next step
-__global__ void k_fix_to_float(unsigned long long* __restrict__ fx, float* __restrict__ rho, long long n) {
-  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const long long v = (long long)fx[k];
-  rho[k] = (float)((double)v * kInvFix);
-  fx[k] = 0ull;
+// Order <= 1 (8-node stencils): every node goes straight into the 64-bit global accumulator.  A
+// shared box would cost more to zero, synchronise and flush than its shared atomics save.
+template <int D, int P>
+__global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict__ pos, const float* __restrict__ charge,
+                                                      const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd,
+                                                      unsigned long long* __restrict__ rho_fx_all, int* status) {
+  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
+  if (!sd.active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float4 p = pos[i];
+  const int t = tild_type_of(p.w);
+  if (t == kPadType) return;
+  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+    atomicOr(status, ST_NONFINITE_POS);
+    return;
+  }
+  const Geom& g = sd.g;
+  const int T = sd.T;
+  const long long M = g.M;
+  const float xs[3] = {p.x, p.y, p.z};
+  float W[3][P + 1];
+  int idx[3][P + 1];
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    const int b = axis_base<P>(xs[d], g.dx[d], W[d]);
+#pragma unroll
+    for (int a = 0; a <= P; a++) idx[d][a] = pmod(b + a, g.nx[d]);
+  }
+  const float q = sd.C ? charge[i] : 0.f;
+  unsigned long long* rt = rho_fx_all + sd.grid0 + (long long)t * M;
+  unsigned long long* rc = rho_fx_all + sd.grid0 + (long long)T * M;
+  const double sc64 = 4294967296.0 / (double)g.gvol;
+#pragma unroll
+  for (int ix = 0; ix <= P; ix++)
+#pragma unroll
+    for (int iy = 0; iy <= P; iy++) {
+      const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
+      const float wxy = W[0][ix] * W[1][iy];
+#pragma unroll
+      for (int iz = 0; iz <= (D == 3 ? P : 0); iz++) {
+        const long long m = D == 3 ? row + (long long)idx[2][iz] * g.nx[1] * g.nx[0] : row;
+        const double W3 = (double)(D == 3 ? wxy * W[2][iz] : wxy) * sc64;
+        atomicAdd(rt + m, (unsigned long long)__double2ll_rn(W3));
+        if (q != 0.f) atomicAdd(rc + m, (unsigned long long)__double2ll_rn(W3 * q));
+      }
+    }
+}
+
+// fixed-point grid -> FP32 density, clearing the accumulator for the next step.  Inactive systems
+// keep the densities of their last force evaluation (their observables still read them).
+__global__ void k_fix_to_float(unsigned long long* __restrict__ fx_all, float* __restrict__ rho_all,
+                               const int* __restrict__ cta_sys, const int* __restrict__ blk0,
+                               const SysDev* __restrict__ sysd) {
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  if (!sd.active) return;
+  const long long M = sd.g.M;
+  const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  const int nch = sd.T + sd.C;
+  for (int ch = 0; ch < nch; ch++) {
+    const long long k = sd.grid0 + (long long)ch * M + m;
+    const long long v = (long long)fx_all[k];
+    rho_all[k] = (float)((double)v * kInvFix);
+    fx_all[k] = 0ull;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -424,6 +481,16 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
   const long long M = g.M;
   const int T = sd.T, C = sd.C;
   const float4* g4 = g4_all + sd.grid0;
+  // loads that do not depend on the stencil are issued before it, so their latency overlaps
+  const int info = bond_info[i];
+  const int nb = info & 3;
+  float4 pj[3];
+#pragma unroll
+  for (int bb = 0; bb < 3; bb++)
+    if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
+  const int bid = bead_id[i];
+  float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
   float f[3] = {0.f, 0.f, 0.f};
   {
     float W[3][P + 1];
@@ -446,13 +513,11 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
     gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
   }
   // bonds
-  const int info = bond_info[i];
-  const int nb = info & 3;
-  for (int bb = 0; bb < nb; bb++) {
-    const int j = bond_nbr[3 * i + bb];
+#pragma unroll
+  for (int bb = 0; bb < 3; bb++) {
+    if (bb >= nb) break;
     const int bt = (info >> (8 + 8 * bb)) & 0xff;
-    const float4 pj = pos_in[j];
-    const float xj[3] = {pj.x, pj.y, pj.z};
+    const float xj[3] = {pj[bb].x, pj[bb].y, pj[bb].z};
     float dr[3], mdr2 = 0.f;
 #pragma unroll
     for (int d = 0; d < D; d++) {
@@ -469,7 +534,6 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
 #pragma unroll
     for (int d = 0; d < D; d++) f[d] -= mf * dr[d];
   }
-  const int bid = bead_id[i];
   if (f_out && s == f_sys) {
 #pragma unroll
     for (int d = 0; d < D; d++) f_out[(long long)bid * D + d] = f[d];
@@ -478,7 +542,6 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
   // integrators in input order (integrator.cu:24-39 is called for each in turn)
   const int mask = sd.type_mask[t];
   const long long est = sd.step + 1;
-  const float4 po = pos_io[i];  // x_{n-1} (GJF xo)
   float xo[3] = {po.x, po.y, po.z};
   float on[3] = {0.f, 0.f, 0.f};
   bool any_gjf = false;
@@ -543,13 +606,22 @@ __global__ void k_hold_inactive(const float4* __restrict__ pos_in, float4* __res
   pos_io[i] = pos_in[i];
 }
 
+// step counters advance on the device; a system whose counter reaches its stop step leaves the
+// active set here, so the next launches skip it without the host in the loop
 __global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < nsys && sysd[s].active) sysd[s].step += 1;
+  if (s >= nsys || !sysd[s].active) return;
+  const long long step = sysd[s].step + 1;
+  sysd[s].step = step;
+  if (sysd[s].stop_at >= 0 && step >= sysd[s].stop_at) sysd[s].active = 0;
 }
 
 template <int D, int P>
 void launch_spread(tild_ctx* c) {
+  if constexpr (P <= 1) {
+    k_spread_direct<D, P><<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
+                                                                   c->rho_fx, c->d_status);
+  } else {
   const size_t smem = sizeof(int) * (size_t)c->spread_cap;
   static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
   if (!(attr_devices >> (c->device & 63) & 1ull)) {
@@ -558,6 +630,7 @@ void launch_spread(tild_ctx* c) {
   }
   k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
                                                                    c->rho_fx, c->spread_cap, c->d_status);
+  }
 }
 
 template <int D, int P, bool I, bool X>
@@ -644,7 +717,8 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (c->D == 3) dispatch_p_spread<3>(c);
   else dispatch_p_spread<2>(c);
   tild_mark(c, STAGE_ZERO);
-  k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
+  k_fix_to_float<<<c->n_cta_grid, 256, 0, c->stream>>>(c->rho_fx, c->rho, c->cta_grid, c->cta_grid + c->n_cta_grid,
+                                                      c->d_sys);
   c->launches += 2;
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);

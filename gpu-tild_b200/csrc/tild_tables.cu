@@ -235,31 +235,19 @@ int tild_build_tables(tild_ctx* c, int si) {
   const int nfft = (int)h.fft_cfg.size();
   // per-direction real slabs start on 16-byte boundaries (cuFFT rejects a misaligned output)
   const long long Mpad = (g.M + 1) / 2 * 2;
-  double* ufull = nullptr;
-  cufftDoubleComplex* zbuf = nullptr;
-  cufftDoubleComplex* zbuf2 = nullptr;
-  double* freal = nullptr;
-  double* vr = nullptr;
-  cufftHandle pz2d = 0, pd2z = 0;
   int rc = TILD_OK;
+  cufftHandle pz2d = 0, pd2z = 0;
   if (nfft > 0) {
-    if (tild_check(c, cudaMalloc(&ufull, sizeof(double) * g.Mh), "alloc ufull") ||
-        tild_check(c, cudaMalloc(&zbuf, sizeof(cufftDoubleComplex) * g.Mh), "alloc zbuf") ||
-        tild_check(c, cudaMalloc(&zbuf2, sizeof(cufftDoubleComplex) * g.Mh), "alloc zbuf2") ||
-        tild_check(c, cudaMalloc(&freal, sizeof(double) * Mpad * D), "alloc freal") ||
-        tild_check(c, cudaMalloc(&vr, sizeof(double) * g.M), "alloc vr")) {
-      rc = TILD_ERR_OOM;
-    }
-    int n[3];
-    if (D == 3) { n[0] = g.nx[2]; n[1] = g.nx[1]; n[2] = g.nx[0]; }
-    else { n[0] = g.nx[1]; n[1] = g.nx[0]; }
-    if (rc == TILD_OK &&
-        (tild_check_fft(c, cufftPlanMany(&pz2d, D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 1), "plan z2d") ||
-         tild_check_fft(c, cufftPlanMany(&pd2z, D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1), "plan d2z") ||
-         tild_check_fft(c, cufftSetStream(pz2d, st), "stream z2d") ||
-         tild_check_fft(c, cufftSetStream(pd2z, st), "stream d2z")))
-      rc = TILD_ERR_CUDA;
+    rc = tild_table_scratch(c);
+    if (rc) return rc;
+    rc = tild_table_plans(c, g, D, &pz2d, &pd2z);
+    if (rc) return rc;
   }
+  double* ufull = c->tab_ufull;
+  cufftDoubleComplex* zbuf = c->tab_z;
+  cufftDoubleComplex* zbuf2 = c->tab_z2;
+  double* freal = c->tab_freal;
+  double* vr = c->tab_vr;
   SysDev& hd = c->h_sys[si];
   for (int s = 0; s < nfft && rc == TILD_OK; s++) {
     const tild_pair_style& ps = h.cfg.styles[h.fft_cfg[s]];
@@ -310,12 +298,73 @@ int tild_build_tables(tild_ctx* c, int si) {
     c->launches++;
   }
   if (rc == TILD_OK && tild_check(c, cudaStreamSynchronize(st), "table build")) rc = TILD_ERR_CUDA;
-  if (pz2d) cufftDestroy(pz2d);
-  if (pd2z) cufftDestroy(pd2z);
-  cudaFree(ufull);
-  cudaFree(zbuf);
-  cudaFree(zbuf2);
-  cudaFree(freal);
-  cudaFree(vr);
   return rc;
+}
+
+// Scratch of the FP64 table builds, sized once for the largest grid of the engine and kept, so
+// that reloading a system (tild_batch_load) allocates nothing.
+int tild_table_scratch(tild_ctx* c) {
+  if (c->tab_ufull) return TILD_OK;
+  long long M = 1, Mh = 1;
+  int D = 3;
+  for (const SysHost& h : c->sys) {
+    M = std::max(M, h.g.M);
+    Mh = std::max(Mh, h.g.Mh);
+    D = h.D;
+  }
+  const long long Mpad = (M + 1) / 2 * 2;
+  if (tild_check(c, cudaMalloc(&c->tab_ufull, sizeof(double) * Mh), "alloc table scratch") ||
+      tild_check(c, cudaMalloc(&c->tab_z, sizeof(cufftDoubleComplex) * Mh), "alloc table scratch") ||
+      tild_check(c, cudaMalloc(&c->tab_z2, sizeof(cufftDoubleComplex) * Mh), "alloc table scratch") ||
+      tild_check(c, cudaMalloc(&c->tab_freal, sizeof(double) * Mpad * D), "alloc table scratch") ||
+      tild_check(c, cudaMalloc(&c->tab_vr, sizeof(double) * M), "alloc table scratch"))
+    return TILD_ERR_OOM;
+  c->tab_M = M;
+  return TILD_OK;
+}
+
+// Z2D / D2Z plans of one grid shape, made once per shape and kept for the engine's lifetime.
+int tild_table_plans(tild_ctx* c, const Geom& g, int D, cufftHandle* z2d, cufftHandle* d2z) {
+  for (const auto& tp : c->tab_plans)
+    if (tp.nx[0] == g.nx[0] && tp.nx[1] == g.nx[1] && tp.nx[2] == g.nx[2]) {
+      *z2d = tp.z2d;
+      *d2z = tp.d2z;
+      return TILD_OK;
+    }
+  int n[3];
+  if (D == 3) { n[0] = g.nx[2]; n[1] = g.nx[1]; n[2] = g.nx[0]; }
+  else { n[0] = g.nx[1]; n[1] = g.nx[0]; }
+  tild_ctx::TablePlan tp;
+  for (int q = 0; q < 3; q++) tp.nx[q] = g.nx[q];
+  tp.z2d = tp.d2z = 0;
+  if (tild_check_fft(c, cufftPlanMany(&tp.z2d, D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 1), "plan z2d"))
+    return TILD_ERR_CUDA;
+  if (tild_check_fft(c, cufftPlanMany(&tp.d2z, D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1), "plan d2z")) {
+    cufftDestroy(tp.z2d);
+    return TILD_ERR_CUDA;
+  }
+  if (tild_check_fft(c, cufftSetStream(tp.z2d, c->stream), "stream z2d") ||
+      tild_check_fft(c, cufftSetStream(tp.d2z, c->stream), "stream d2z")) {
+    cufftDestroy(tp.z2d);
+    cufftDestroy(tp.d2z);
+    return TILD_ERR_CUDA;
+  }
+  c->tab_plans.push_back(tp);
+  *z2d = tp.z2d;
+  *d2z = tp.d2z;
+  return TILD_OK;
+}
+
+void tild_tables_free(tild_ctx* c) {
+  for (auto& tp : c->tab_plans) {
+    cufftDestroy(tp.z2d);
+    cufftDestroy(tp.d2z);
+  }
+  c->tab_plans.clear();
+  void* ptrs[] = {c->tab_ufull, c->tab_z, c->tab_z2, c->tab_freal, c->tab_vr};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->tab_ufull = nullptr;
+  c->tab_z = c->tab_z2 = nullptr;
+  c->tab_freal = c->tab_vr = nullptr;
 }

@@ -108,6 +108,10 @@ def lib() -> C.CDLL:
         "tild_batch_forces": ([vp, i32, fp], i32), "tild_batch_observables": ([vp, i32, C.POINTER(Obs)], i32),
         "tild_batch_get_density": ([vp, i32, fp], i32), "tild_batch_time_steps": ([vp, i32, dp], i32),
         "tild_batch_sync": ([vp], i32),
+        "tild_batch_sk_accumulate": ([vp, i32, i32, i32], i32), "tild_batch_sk_get": ([vp, i32, i32, dp, ip], i32),
+        "tild_batch_create_slots": ([C.POINTER(Config), ip, i32, i32, C.POINTER(vp)], i32),
+        "tild_batch_capacity": ([vp, i32, ip], i32), "tild_batch_load": ([vp, i32, C.POINTER(Config)], i32),
+        "tild_batch_set_stop": ([vp, i32, C.c_int64], i32), "tild_batch_get_active": ([vp, i32, ip], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -367,13 +371,21 @@ class Batch:
     """Many independent systems advanced together (a tild_batch): one launch per stage for all
     systems, one batched cuFFT plan per grid shape.  Systems share dim, pmeorder and rng."""
 
-    def __init__(self, systems: Sequence[System], device: int = 0):
+    def __init__(self, systems: Sequence[System], device: int = 0, capacity: Optional[Sequence[int]] = None):
+        """capacity: beads reserved per system (a slot batch, tild_batch_create_slots), so that
+        load() can later put another system of the same grid shape into that slot."""
         L = lib()
         self.systems = list(systems)
         n = len(self.systems)
         self._cfgs = (Config * n)(*[s.config() for s in self.systems])
         h = C.c_void_p()
-        st = L.tild_batch_create(self._cfgs, n, device, C.byref(h))
+        if capacity is None:
+            st = L.tild_batch_create(self._cfgs, n, device, C.byref(h))
+        else:
+            cap = np.ascontiguousarray(capacity, dtype=np.int32)
+            if cap.shape != (n,):
+                raise ValueError("one capacity per system")
+            st = L.tild_batch_create_slots(self._cfgs, _ptr(cap, C.c_int32), n, device, C.byref(h))
         if st != OK:
             raise TildError(st, f"tild_batch_create failed: {L.tild_status_string(st).decode()}")
         self._h = h
@@ -477,3 +489,40 @@ class Batch:
 
     def sync(self):
         self._check(lib().tild_batch_sync(self._h), "tild_batch_sync")
+
+    # ---- avg_sk per system ----
+    def sk_accumulate(self, i: int, slot: int, type_: int):
+        self._check(lib().tild_batch_sk_accumulate(self._h, i, slot, type_), "tild_batch_sk_accumulate")
+
+    def sk_get(self, i: int, slot: int):
+        s = self.systems[i]
+        out = np.empty(2 * int(np.prod(s.nx[:s.dim])), np.float64)
+        n = C.c_int32()
+        self._check(lib().tild_batch_sk_get(self._h, i, slot, _ptr(out, C.c_double), C.byref(n)), "tild_batch_sk_get")
+        return out.view(np.complex128), n.value
+
+    # ---- slots (continuous batching) ----
+    def capacity(self, i: int) -> int:
+        v = C.c_int32()
+        self._check(lib().tild_batch_capacity(self._h, i, C.byref(v)), "tild_batch_capacity")
+        return v.value
+
+    def load(self, i: int, s: System, activate: bool = True):
+        """Put system s into slot i (same grid shape and channel layout, s.ns <= capacity):
+        tables rebuilt, topology and state uploaded, step counter 0."""
+        cfg = s.config()
+        self._check(lib().tild_batch_load(self._h, i, C.byref(cfg)), "tild_batch_load")
+        self._cfgs[i] = cfg
+        self.systems[i] = s
+        self.set_topology(i, s)
+        self.set_state(i, s.x)
+        if activate:
+            self.set_active(i, True)
+
+    def set_stop(self, i: int, stop_at: int):
+        self._check(lib().tild_batch_set_stop(self._h, i, int(stop_at)), "tild_batch_set_stop")
+
+    def active(self, i: int) -> bool:
+        v = C.c_int32()
+        self._check(lib().tild_batch_get_active(self._h, i, C.byref(v)), "tild_batch_get_active")
+        return bool(v.value)

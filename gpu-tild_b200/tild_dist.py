@@ -63,6 +63,14 @@ class Group:
     def sum(self, v: float) -> float:
         return self._reduce(v, None if self.dist is None else self.dist.ReduceOp.SUM)
 
+    def gather_lists(self, items: list) -> list:
+        """Concatenation of every rank's list (all ranks receive it)."""
+        if self.dist is None:
+            return list(items)
+        out = [None] * self.world
+        self.dist.all_gather_object(out, list(items))
+        return [x for part in out for x in part]
+
     def close(self):
         if self.dist is not None:
             self.dist.destroy_process_group()

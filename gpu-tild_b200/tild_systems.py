@@ -162,6 +162,27 @@ def ensemble_member(index: int, base_seed: int = SEED_BASE + 3, dx: float = 0.5,
                         seed=base_seed + 100000 + index, max_steps=5000)
 
 
+def ensemble_grid_edges(dx: float = 0.5):
+    """Grid edges the batched-ensemble distribution can draw: round(U(12, 24) / dx)."""
+    return list(range(int(round(12.0 / dx)), int(round(24.0 / dx)) + 1))
+
+
+def ensemble_capacity(g: int, dx: float = 0.5, rho0: float = 5.0, n_max: int = 40) -> int:
+    """Largest bead count an ensemble member on a g^3 grid can have: round(rho0 L^3 / N) * N
+    <= rho0 L^3 + N / 2 for every chain length N <= n_max."""
+    L = g * dx
+    return int(math.floor(rho0 * L ** 3 + n_max / 2)) + 1
+
+
+def ensemble_slot_template(g: int, dx: float = 0.5, rho0: float = 5.0, seed: int = SEED_BASE + 7) -> System:
+    """A placeholder diblock system of grid g^3 (same channel layout as every ensemble member)
+    that initialises one slot of a serving batch before its first job arrives."""
+    L = g * dx
+    N = 20
+    return diblock_melt(n_chains=max(1, int(round(rho0 * L ** 3 / N))), N=N, fA=0.5, box=(L, L, L), nx=(g, g, g),
+                        kappa=50.0, chiN=20.0, seed=seed + g, max_steps=5000)
+
+
 # ------------------------------------------------------------------------------------------
 # reference file formats
 # ------------------------------------------------------------------------------------------

@@ -247,6 +247,29 @@ int32_t tild_batch_observables(tild_batch* b, int32_t sys, tild_obs* out);
 int32_t tild_batch_get_density(tild_batch* b, int32_t sys, float* rho);
 int32_t tild_batch_time_steps(tild_batch* b, int32_t nsteps, double* ms);
 int32_t tild_batch_sync(tild_batch* b);
+/* avg_sk of one system (tild_sk_accumulate / tild_sk_get for system `sys`). */
+int32_t tild_batch_sk_accumulate(tild_batch* b, int32_t sys, int32_t slot, int32_t type);
+int32_t tild_batch_sk_get(tild_batch* b, int32_t sys, int32_t slot, double* sk, int32_t* ncalls);
+
+/* ---- slots: continuous batching (no reference counterpart) ----------------------------------- */
+/* A slot batch reserves capacity[s] >= cfgs[s].ns beads for system s, so that tild_batch_load can
+ * later put another system of the same grid shape into slot s while the others keep running. */
+int32_t tild_batch_create_slots(const tild_config* cfgs, const int32_t* capacity, int32_t nsys, int32_t device,
+                                tild_batch** out);
+int32_t tild_batch_capacity(tild_batch* b, int32_t sys, int32_t* capacity);
+/* Replaces the system of slot `sys` by cfg.  cfg must share the slot's dim, pmeorder, rng, grid
+ * nx, ntypes and do_charges, and its number of FFT pair styles and of fieldphase styles, with
+ * cfg->ns <= the slot's capacity; box, style parameters, bonds, masses, integrators, seed, time
+ * step and max_steps may differ.  The slot's k-space tables are rebuilt (nothing is allocated),
+ * its avg_sk accumulators are cleared, its step counter is 0 and it is left inactive without
+ * topology or state: tild_batch_set_topology, tild_batch_set_state and tild_batch_set_active
+ * follow.  Waits for the batch's stream. */
+int32_t tild_batch_load(tild_batch* b, int32_t sys, const tild_config* cfg);
+/* System `sys` leaves the active set on the device when its step counter reaches stop_at
+ * (-1: never), so a stepping call may run past a system's last step: that system takes exactly
+ * stop_at - step steps.  Step counters and activity are read back after every stepping call. */
+int32_t tild_batch_set_stop(tild_batch* b, int32_t sys, int64_t stop_at);
+int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active);
 
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (code that

@@ -1,0 +1,119 @@
+"""Request loop of the serving layer, on the host: admission by grid shape and free slots, first
+come first served, device-side stops, retirement and the latency summary.  The slot batch is a
+host stand-in with the same interface (no GPU): steps advance counters, a slot leaves the active
+set when its counter reaches the stop step, exactly as k_advance_steps does."""
+import numpy as np
+
+import tild_serve as sv
+import tild_systems as ts
+
+
+class FakeBatch:
+    def __init__(self, systems, caps):
+        self.systems = list(systems)
+        self.caps = list(caps)
+        self.stepc = [0] * len(systems)
+        self.act = [True] * len(systems)
+        self.stop = [-1] * len(systems)
+        self.loads = []
+        self.sk = [0] * len(systems)
+
+    def sync(self):
+        pass
+
+    def close(self):
+        pass
+
+    def set_active(self, i, a):
+        assert not a or self.stop[i] < 0 or self.stepc[i] < self.stop[i]
+        self.act[i] = bool(a)
+
+    def load(self, i, s, activate=True):
+        assert s.ns <= self.caps[i]
+        assert tuple(s.nx) == tuple(self.systems[i].nx)
+        self.systems[i] = s
+        self.stepc[i] = 0
+        self.stop[i] = -1
+        self.sk[i] = 0
+        self.act[i] = bool(activate)
+        self.loads.append(i)
+
+    def set_stop(self, i, n):
+        self.stop[i] = n
+
+    def step(self, n):
+        for _ in range(n):
+            for i in range(len(self.systems)):
+                if self.act[i]:
+                    self.stepc[i] += 1
+                    if self.stop[i] >= 0 and self.stepc[i] >= self.stop[i]:
+                        self.act[i] = False
+
+    def observables(self, i):
+        return {"upe": float(self.stepc[i]) + 0.5 * i}
+
+    def step_count(self, i):
+        return self.stepc[i]
+
+    def sk_accumulate(self, i, slot, t):
+        self.sk[i] += 1
+
+    def active(self, i):
+        return self.act[i]
+
+    def sk_get(self, i, slot):
+        return np.zeros(4, np.complex128), self.sk[i]
+
+
+class FakeServer(sv.Server):
+    def _make_batch(self, systems, caps):
+        return FakeBatch(systems, caps)
+
+
+def tiny(g, seed):
+    L = g * 0.5
+    return ts.diblock_melt(n_chains=6, N=10, box=(L, L, L), nx=(g, g, g), seed=seed)
+
+
+def test_fifo_admission_per_grid_shape_and_device_stops():
+    srv = FakeServer({24: 1, 26: 2}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                     measure_memory=False)
+    jobs = [sv.Job(0, tiny(24, 2), 100, 0), sv.Job(1, tiny(24, 3), 64, 0), sv.Job(2, tiny(26, 4), 200, 1),
+            sv.Job(3, tiny(26, 5), 10, 1), sv.Job(4, tiny(26, 6), 64, 5)]
+    res = srv.run(jobs, clock="epochs")
+    by = {r.job_id: r for r in res}
+    # job 1 waits for job 0's slot (one edge-24 slot): 0 needs two epochs (100 steps, epoch 64)
+    assert by[0].admitted == 0 and by[0].finished == 2
+    assert by[1].admitted == 2 and by[1].finished == 3
+    # both edge-26 jobs start at epoch 1; the 10-step job retires after one epoch
+    assert by[2].admitted == 1 and by[3].admitted == 1 and by[3].finished == 2
+    assert by[2].finished == 5
+    # job 4 arrives at epoch 5 to a free slot
+    assert by[4].admitted == 5 and by[4].finished == 6
+    for r in res:
+        steps = [s for s, _ in r.energy]
+        assert steps[-1] == r.steps                                 # the last record is the stop step
+        assert steps == sorted(steps) and len(steps) == -(-r.steps // 64)
+        assert r.sk_calls == len(steps)
+    summ = sv.latency_summary(res)
+    assert summ["jobs"] == 5 and summ["p99_s"] >= summ["p50_s"] > 0
+
+
+def test_job_without_slot_shape_is_rejected():
+    srv = FakeServer({24: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), measure_memory=False)
+    try:
+        srv.run([sv.Job(0, tiny(30, 2), 10, 0)], clock="epochs")
+    except ValueError as e:
+        assert "grid edge 30" in str(e)
+    else:
+        raise AssertionError("a job without a slot of its grid shape must be rejected")
+
+
+def test_poisson_stream_and_capacity():
+    jobs = sv.poisson_jobs(8, rate=50.0, steps=5000, seed=3)
+    t = np.array([j.arrival for j in jobs])
+    assert t[0] == 0 and np.all(np.diff(t) > 0)
+    for j in jobs:
+        g = sv.grid_edge(j.system)
+        assert g in ts.ensemble_grid_edges()
+        assert j.system.ns <= ts.ensemble_capacity(g)
