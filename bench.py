@@ -56,6 +56,7 @@ def run_ensemble(args):
     mine = tild_dist.shard([s.ns for s in systems], grp.rank, grp.world)
     local = [systems[i] for i in mine]
     B = tild.Batch(local, device=grp.local)
+    schedule = None if args.no_tune else B.autotune(trial_steps=64)
     B.step(args.warmup * 32)
     B.sync()
     grp.barrier()
@@ -72,7 +73,8 @@ def run_ensemble(args):
            "data": "synthetic (seeded random-walk chains)",
            "config": {"workload": f"ensemble_{args.nsys}_diblock_24^3-48^3_gaussian_p1_GJF",
                       "systems": args.nsys, "beads_total": sum(s.ns for s in systems),
-                      "grid_points_total": int(sum(np.prod(s.nx) for s in systems)), "parallelism": f"shards{grp.world}"},
+                      "grid_points_total": int(sum(np.prod(s.nx) for s in systems)), "parallelism": f"shards{grp.world}",
+                      "schedule": schedule},
            "clocks": clk.summary(), "stages_ms_per_step": {k: v / args.steps for k, v in prof.items()}}
     if grp.rank == 0 and not args.no_serial:
         # one at a time: every 16th system alone, scaled to all systems by their bead counts
@@ -106,8 +108,9 @@ def run_serving(args):
     mine = [j for k, j in enumerate(jobs_all) if k % grp.world == grp.rank]
     # each rank replays its share of the stream: arrivals keep their absolute times
     edges = {g: args.slots_per_edge for g in ts.ensemble_grid_edges()}
-    with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch) as srv:
-        pool_bytes, nslots = srv.pool_bytes, srv.nslots
+    with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch,
+                   tune=not args.no_tune) as srv:
+        pool_bytes, nslots, schedule = srv.pool_bytes, srv.nslots, srv.schedule
         grp.barrier()
         res = srv.run(mine, clock="wall")
         stepping_s = srv.stepping_s
@@ -124,6 +127,7 @@ def run_serving(args):
            "config": {"workload": f"serving_poisson{args.rate:g}_{args.jobs}jobs_{args.job_steps}steps",
                       "slots": nslots * grp.world, "slots_per_edge": args.slots_per_edge, "epoch_steps": args.epoch,
                       "hbm_budget_gb": args.hbm_budget / 1e9, "pool_gb_per_gpu": pool_bytes / 1e9,
+                      "schedule": schedule,
                       "parallelism": f"replicas{grp.world}"},
            "latency": summ,
            "offered_particle_steps_per_s": offered,
@@ -231,7 +235,7 @@ class ClockSampler:
         if shutil.which("nvidia-smi"):
             self.out = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.out,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         return self
 
@@ -271,6 +275,7 @@ def run_ours(args):
     rank, local, ws = grp.rank, grp.local, grp.world
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
+    schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
     ctx.step(args.warmup)
     ctx.sync()
     grp.barrier()
@@ -322,7 +327,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded random-walk chains)",
         "config": {"workload": wname, "ns_per_gpu": s.ns, "grid": list(s.nx[:s.dim]), "pmeorder": s.pmeorder,
                    "pair_styles": len(s.styles), "integrator": "GJF" if s.integrators[0][0] else "EM",
-                   "parallelism": f"replicas{ws}",
+                   "parallelism": f"replicas{ws}", "schedule": schedule,
                    "l2": "per-step working set (positions, grids, spectra) exceeds the 126 MB L2"},
         "clocks": clocks,
         "e2e": e2e,
@@ -412,7 +417,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate", "ensemble", "serving"])
@@ -424,6 +429,7 @@ def main():
     ap.add_argument("--epoch", type=int, default=128)
     ap.add_argument("--hbm-budget", type=float, default=80e9)
     ap.add_argument("--serial-sample", type=int, default=6)
+    ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner")
     ap.add_argument("--no-serial", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")

@@ -181,6 +181,43 @@ int spread_kbits(int P, int D, double gvol, double qmax) {
   return k;
 }
 
+}  // namespace
+
+// Spreads the grid-shape buckets over the first `lanes` auxiliary streams (largest first, each to
+// the least loaded stream) and binds their cuFFT plans to them; lanes = 0 keeps every transform on
+// the main stream.
+int tild_assign_lanes(tild_ctx* c, int lanes) {
+  lanes = std::max(0, std::min(lanes, (int)c->aux.size()));
+  std::vector<int> order(c->buckets.size());
+  for (size_t k = 0; k < order.size(); k++) order[k] = (int)k;
+  auto work = [&](int k) {
+    const Bucket& b = c->buckets[k];
+    return (long long)b.nx[0] * b.nx[1] * b.nx[2] * b.channels;
+  };
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  std::vector<long long> load(std::max(lanes, 1), 0);
+  for (int bi : order) {
+    Bucket& b = c->buckets[bi];
+    if (lanes == 0) {
+      b.lane = -1;
+    } else {
+      int best = 0;
+      for (int k = 1; k < lanes; k++)
+        if (load[k] < load[best]) best = k;
+      b.lane = best;
+      load[best] += work(bi);
+    }
+    if (!b.planned) continue;
+    cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
+    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, bs), "plan stream"))
+      return 1;
+  }
+  c->lanes = lanes;
+  return 0;
+}
+
+namespace {
+
 // Geometry of a system from its configuration (initialize.cu:30-60).
 void set_geometry(SysHost& h, const tild_config& cfg) {
   h.D = cfg.dim;
@@ -445,25 +482,6 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
         return TILD_ERR_CUDA;
     }
     if (tild_check(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "fork event")) return TILD_ERR_CUDA;
-    // largest buckets first, each to the least loaded stream
-    std::vector<int> order(c->buckets.size());
-    for (size_t k = 0; k < order.size(); k++) order[k] = (int)k;
-    std::sort(order.begin(), order.end(), [&](int a, int b) {
-      const Bucket& A = c->buckets[a];
-      const Bucket& B = c->buckets[b];
-      return (long long)A.nx[0] * A.nx[1] * A.nx[2] * A.channels > (long long)B.nx[0] * B.nx[1] * B.nx[2] * B.channels;
-    });
-    std::vector<long long> load(naux, 0);
-    for (int bi : order) {
-      int best = 0;
-      for (int k = 1; k < naux; k++)
-        if (load[k] < load[best]) best = k;
-      Bucket& b = c->buckets[bi];
-      b.lane = best;
-      load[best] += (long long)b.nx[0] * b.nx[1] * b.nx[2] * b.channels;
-    }
-  } else {
-    c->buckets[0].lane = -1;
   }
   for (Bucket& b : c->buckets) {
     int n[3];
@@ -476,10 +494,8 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
       return TILD_ERR_CUDA;
     }
     b.planned = true;
-    cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : st;
-    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, bs), "plan stream"))
-      return TILD_ERR_CUDA;
   }
+  if (tild_assign_lanes(c, (int)c->aux.size())) return TILD_ERR_CUDA;
   for (int s = 0; s < nsys && !rc; s++) rc = tild_build_tables(c, s);
   if (rc) return rc;
   if (c->sort_interval > 0) {
@@ -885,6 +901,135 @@ int sys_sk_get(tild_ctx* c, int s, int slot, double* sk, int32_t* ncalls) {
   return TILD_OK;
 }
 
+void drop_graphs(tild_ctx* c) {
+  for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+  c->graphs.clear();
+}
+
+// ---- schedule tuning -------------------------------------------------------------------------
+void get_tune(const tild_ctx* c, tild_tune* t) {
+  t->spread_mode = c->spread_mode;
+  t->spread_cap = c->spread_cap;
+  t->sort_interval = c->sort_interval;
+  t->fft_streams = c->lanes;
+  t->ms_per_step = 0.0;
+}
+
+int set_tune(tild_ctx* c, const tild_tune* t) {
+  if (!t || (t->spread_mode != TILD_SPREAD_TILED && t->spread_mode != TILD_SPREAD_DIRECT) || t->spread_cap < 1024 ||
+      t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8)
+    return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
+  if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
+  cudaSetDevice(c->device);
+  if (tild_check(c, cudaStreamSynchronize(c->stream), "sync before tune")) return TILD_ERR_CUDA;
+  c->spread_mode = t->spread_mode;
+  c->spread_cap = t->spread_cap;
+  if (t->sort_interval != c->sort_interval) {
+    c->sort_interval = t->sort_interval;
+    c->steps_since_sort = c->sort_interval;
+  }
+  if (tild_assign_lanes(c, t->fft_streams)) return TILD_ERR_CUDA;
+  // captured graphs hold the old launches
+  for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
+  c->graphs.clear();
+  return TILD_OK;
+}
+
+int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
+  if (!c || trial_steps < 1) return TILD_ERR_BAD_INPUT;
+  if (c->rng == TILD_RNG_XORWOW) return set_err(c, TILD_ERR_UNSUPPORTED, "autotuning would advance the cuRAND states");
+  if (!all_ready(c)) return set_err(c, TILD_ERR_STATE, "no state");
+  cudaSetDevice(c->device);
+  // snapshot every system with a state
+  struct Snap {
+    std::vector<float> x, xo, nz;
+    int64_t step;
+    bool active;
+  };
+  std::vector<Snap> snap(c->nsys);
+  for (int s = 0; s < c->nsys; s++) {
+    SysHost& h = c->sys[s];
+    snap[s].step = h.step;
+    snap[s].active = h.active;
+    if (!h.state_set) continue;
+    const size_t n = (size_t)h.ns * h.D;
+    snap[s].x.resize(n);
+    snap[s].xo.resize(n);
+    snap[s].nz.resize(n);
+    int rc = sys_get_state(c, s, snap[s].x.data(), snap[s].xo.data(), snap[s].nz.data());
+    if (rc) return rc;
+  }
+  const bool use_graphs = c->use_graphs;
+  int rc = TILD_OK;
+  auto trial = [&](const tild_tune& t, double* ms) -> int {
+    int r = set_tune(c, &t);
+    if (r) return r;
+    const int period = c->sort_interval > 0 ? 2 * c->sort_interval : c->graph_len;
+    r = run_steps(c, period);  // warm-up (and graph capture)
+    if (r) return r;
+    return engine_time(c, trial_steps, ms);
+  };
+  tild_tune cur;
+  get_tune(c, &cur);
+  double cur_ms = 0.0;
+  rc = trial(cur, &cur_ms);
+  auto consider = [&](tild_tune t) {
+    if (rc) return;
+    double ms = 0.0;
+    rc = trial(t, &ms);
+    if (!rc && ms < cur_ms) {
+      cur = t;
+      cur_ms = ms;
+    }
+  };
+  if (c->P >= 2) {
+    for (int mode : {TILD_SPREAD_TILED, TILD_SPREAD_DIRECT}) {
+      tild_tune t = cur;
+      t.spread_mode = mode;
+      if (mode != cur.spread_mode) consider(t);
+    }
+    if (cur.spread_mode == TILD_SPREAD_TILED)
+      for (int cap : {3072, 6144, 12288}) {
+        tild_tune t = cur;
+        t.spread_cap = cap;
+        if (cap != cur.spread_cap) consider(t);
+      }
+  }
+  if (c->sort_temp)
+    for (int si : {8, 16, 32}) {
+      tild_tune t = cur;
+      t.sort_interval = si;
+      if (si != cur.sort_interval) consider(t);
+    }
+  if (!c->aux.empty())
+    for (int l : {0, 2, 4, 8}) {
+      tild_tune t = cur;
+      t.fft_streams = std::min<int>(l, (int)c->aux.size());
+      if (t.fft_streams != cur.fft_streams) consider(t);
+    }
+  const int rc_trials = rc;
+  // keep the fastest, then put every system back where it was
+  rc = set_tune(c, &cur);
+  for (int s = 0; s < c->nsys && !rc; s++) {
+    SysHost& h = c->sys[s];
+    h.active = snap[s].active;
+    if (!snap[s].x.empty()) rc = sys_set_state(c, s, snap[s].x.data(), snap[s].xo.data(), snap[s].nz.data());
+    if (!rc) {
+      h.step = snap[s].step;
+      c->h_sys[s].step = snap[s].step;
+    }
+  }
+  if (!rc) rc = tild_upload_sys(c);
+  c->use_graphs = use_graphs;
+  if (rc_trials) return rc_trials;
+  if (rc) return rc;
+  if (best) {
+    *best = cur;
+    best->ms_per_step = cur_ms / trial_steps;
+  }
+  return TILD_OK;
+}
+
 }  // namespace
 
 struct tild_batch : public tild_ctx {};
@@ -1127,6 +1272,19 @@ int32_t tild_batch_create_slots(const tild_config* cfgs, const int32_t* capacity
   return create_common(cfgs, nsys, device, out, capacity);
 }
 int32_t tild_batch_load(tild_batch* b, int32_t sys, const tild_config* cfg) { return sys_load(b, sys, cfg); }
+int32_t tild_autotune(tild_ctx* c, int32_t trial_steps, tild_tune* best) { return engine_autotune(c, trial_steps, best); }
+int32_t tild_get_tune(tild_ctx* c, tild_tune* out) {
+  if (!c || !out) return TILD_ERR_BAD_INPUT;
+  get_tune(c, out);
+  return TILD_OK;
+}
+int32_t tild_set_tune(tild_ctx* c, const tild_tune* t) {
+  if (!c) return TILD_ERR_BAD_INPUT;
+  return set_tune(c, t);
+}
+int32_t tild_batch_autotune(tild_batch* b, int32_t trial_steps, tild_tune* best) { return engine_autotune(b, trial_steps, best); }
+int32_t tild_batch_get_tune(tild_batch* b, tild_tune* out) { return tild_get_tune(b, out); }
+int32_t tild_batch_set_tune(tild_batch* b, const tild_tune* t) { return tild_set_tune(b, t); }
 int32_t tild_batch_capacity(tild_batch* b, int32_t sys, int32_t* capacity) {
   if (check_sys(b, sys) || !capacity) return TILD_ERR_BAD_INPUT;
   *capacity = b->sys[sys].cap;
@@ -1135,7 +1293,11 @@ int32_t tild_batch_capacity(tild_batch* b, int32_t sys, int32_t* capacity) {
 int32_t tild_batch_set_stop(tild_batch* b, int32_t sys, int64_t stop_at) {
   if (check_sys(b, sys) || stop_at < -1) return TILD_ERR_BAD_INPUT;
   b->h_sys[sys].stop_at = stop_at;
-  if (stop_at >= 0) b->any_stop = true;
+  if (stop_at >= 0 && !b->any_stop) {
+    const bool hold_before = tild_needs_hold(b);
+    b->any_stop = true;
+    if (!hold_before) drop_graphs(b);
+  }
   return tild_upload_sys(b);
 }
 int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active) {
@@ -1165,7 +1327,9 @@ int32_t tild_batch_set_active(tild_batch* b, int32_t sys, int32_t active) {
   if (check_sys(b, sys)) return TILD_ERR_BAD_INPUT;
   if (active && b->h_sys[sys].stop_at >= 0 && b->sys[sys].step >= b->h_sys[sys].stop_at)
     return set_err(b, TILD_ERR_STATE, "the system is at or past its stop step");
+  const bool hold_before = tild_needs_hold(b);
   b->sys[sys].active = active != 0;
+  if (!hold_before && tild_needs_hold(b)) drop_graphs(b);
   return tild_upload_sys(b);
 }
 int32_t tild_batch_set_step(tild_batch* b, int32_t sys, int64_t step) { return sys_set_step(b, sys, step); }

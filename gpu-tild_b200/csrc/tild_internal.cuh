@@ -116,6 +116,9 @@ struct tild_ctx {
   std::vector<cudaStream_t> aux;
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_join;
+  int lanes = 0;                         // auxiliary streams in use (tild_assign_lanes)
+  // tunables (tild_autotune): spread kernel for order >= 2 and its shared box, in 32-bit words
+  int spread_mode = TILD_SPREAD_TILED;
   int D = 3, P = 1;
   int nsys = 1;
   std::vector<SysHost> sys;
@@ -355,6 +358,17 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   //
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);
+int tild_assign_lanes(tild_ctx* c, int lanes);
+
+// Whether a step must carry k_hold_inactive (a system may be inactive while others step).
+// Several systems, a device-side stop or an inactive system make it so; captured graphs are
+// dropped when this turns true.
+inline bool tild_needs_hold(const tild_ctx* c) {
+  if (c->nsys > 1 || c->any_stop) return true;
+  for (const SysHost& h : c->sys)
+    if (!h.active) return true;
+  return false;
+}
 int tild_table_plans(tild_ctx* c, const Geom& g, int D, cufftHandle* z2d, cufftHandle* d2z);
 void tild_tables_free(tild_ctx* c);
 int tild_stencil_run(tild_ctx* c, int s, int* inds_dev, float* w_dev);

@@ -81,6 +81,31 @@ __device__ __forceinline__ void chunk_origin(const float4* __restrict__ pos, int
   __syncthreads();
 }
 
+// One bead's stencil added to the 64-bit global accumulator (2^32 per unit) in contributions
+// rounded at 2^kbits per unit, with the float operations of the shared-box path, so that a node's
+// integer sum is the same whichever path (or spread kernel) a bead takes.
+template <int D, int P>
+__device__ __forceinline__ void spread_global_kbits(const float (&W)[3][P + 1], const int (&idx)[3][P + 1],
+                                                    const Geom& g, unsigned long long* rt, unsigned long long* rc,
+                                                    float q, float ig, int kbits) {
+  const float sc32 = ig * __int_as_float((127 + kbits) << 23);  // 2^kbits / gvol
+  const int sh = 32 - kbits;
+#pragma unroll
+  for (int ix = 0; ix <= P; ix++)
+#pragma unroll
+    for (int iy = 0; iy <= P; iy++) {
+      const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
+      const float wxy = W[0][ix] * W[1][iy] * sc32;
+#pragma unroll
+      for (int iz = 0; iz <= (D == 3 ? P : 0); iz++) {
+        const long long m = D == 3 ? row + (long long)idx[2][iz] * g.nx[1] * g.nx[0] : row;
+        const float W3 = D == 3 ? wxy * W[2][iz] : wxy;
+        atomicAdd(rt + m, (unsigned long long)((long long)__float2int_rn(W3) << sh));
+        if (rc) atomicAdd(rc + m, (unsigned long long)((long long)__float2int_rn(W3 * q) << sh));
+      }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Spreading: d_charge_grid / d_charge_grid_charges (device_grid_utils.cu:111-343)
 // ---------------------------------------------------------------------------------------------
@@ -101,8 +126,7 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   extern __shared__ int smi[];
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ long long s_row[kMaxRows];
-  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
-  if (!sd.active) return;
+  const SysDev& sd = sysd[cta_sys[blockIdx.x]];  // inactive systems too (see k_fix_to_float)
   const Geom g = sd.g;
   const int T = sd.T, C = sd.C, kbits = sd.kbits;
   unsigned long long* rho_fx = rho_fx_all + sd.grid0;
@@ -200,45 +224,26 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
       }
     }
   } else if (ok) {
+    // the box does not fit: the same 2^kbits contributions, added to the global grid directly
     int idx[3][P + 1];
 #pragma unroll
     for (int d = 0; d < D; d++)
 #pragma unroll
       for (int a = 0; a <= P; a++) idx[d][a] = pmod(s_g0[d] + rel[d] + a, g.nx[d]);
-    unsigned long long* rt = rho_fx + (long long)t * M;
-    unsigned long long* rc = rho_fx + (long long)T * M;
-    const double sc64 = 4294967296.0 / (double)g.gvol;
-#pragma unroll
-    for (int ix = 0; ix <= P; ix++)
-#pragma unroll
-      for (int iy = 0; iy <= P; iy++) {
-        const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
-        const float wxy = W[0][ix] * W[1][iy];
-        if (D == 3) {
-#pragma unroll
-          for (int iz = 0; iz <= P; iz++) {
-            const long long m = row + (long long)idx[2][iz] * g.nx[1] * g.nx[0];
-            const double W3 = (double)(wxy * W[2][iz]) * sc64;
-            atomicAdd(rt + m, (unsigned long long)__double2ll_rn(W3));
-            if (qc) atomicAdd(rc + m, (unsigned long long)__double2ll_rn(W3 * q));
-          }
-        } else {
-          const double W3 = (double)wxy * sc64;
-          atomicAdd(rt + row, (unsigned long long)__double2ll_rn(W3));
-          if (qc) atomicAdd(rc + row, (unsigned long long)__double2ll_rn(W3 * q));
-        }
-      }
+    spread_global_kbits<D, P>(W, idx, g, rho_fx + (long long)t * M, qc ? rho_fx + (long long)T * M : nullptr, q,
+                              ig, kbits);
   }
 }
 
-// Order <= 1 (8-node stencils): every node goes straight into the 64-bit global accumulator.  A
-// shared box would cost more to zero, synchronise and flush than its shared atomics save.
+// Every node straight into the 64-bit global accumulator.  For order <= 1 (8-node stencils) a
+// shared box would cost more to zero, synchronise and flush than its shared atomics save, and the
+// contributions keep 2^32 per unit; for higher orders it is the tuner's alternative to the box
+// and rounds contributions exactly as the box does.
 template <int D, int P>
 __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict__ pos, const float* __restrict__ charge,
                                                       const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd,
                                                       unsigned long long* __restrict__ rho_fx_all, int* status) {
-  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
-  if (!sd.active) return;
+  const SysDev& sd = sysd[cta_sys[blockIdx.x]];  // inactive systems too (see k_fix_to_float)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const float4 p = pos[i];
   const int t = tild_type_of(p.w);
@@ -262,6 +267,10 @@ __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict_
   const float q = sd.C ? charge[i] : 0.f;
   unsigned long long* rt = rho_fx_all + sd.grid0 + (long long)t * M;
   unsigned long long* rc = rho_fx_all + sd.grid0 + (long long)T * M;
+  if (P >= 2) {  // same contributions as the shared-box kernel: results independent of the choice
+    spread_global_kbits<D, P>(W, idx, g, rt, q != 0.f ? rc : nullptr, q, 1.0f / g.gvol, sd.kbits);
+    return;
+  }
   const double sc64 = 4294967296.0 / (double)g.gvol;
 #pragma unroll
   for (int ix = 0; ix <= P; ix++)
@@ -279,24 +288,15 @@ __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict_
     }
 }
 
-// fixed-point grid -> FP32 density, clearing the accumulator for the next step.  Inactive systems
-// keep the densities of their last force evaluation (their observables still read them).
-__global__ void k_fix_to_float(unsigned long long* __restrict__ fx_all, float* __restrict__ rho_all,
-                               const int* __restrict__ cta_sys, const int* __restrict__ blk0,
-                               const SysDev* __restrict__ sysd) {
-  const int s = cta_sys[blockIdx.x];
-  const SysDev& sd = sysd[s];
-  if (!sd.active) return;
-  const long long M = sd.g.M;
-  const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
-  if (m >= M) return;
-  const int nch = sd.T + sd.C;
-  for (int ch = 0; ch < nch; ch++) {
-    const long long k = sd.grid0 + (long long)ch * M + m;
-    const long long v = (long long)fx_all[k];
-    rho_all[k] = (float)((double)v * kInvFix);
-    fx_all[k] = 0ull;
-  }
+// fixed-point grid -> FP32 density over every system's channels, clearing the accumulator for the
+// next step.  Inactive systems are spread too (their positions are held), so their densities stay
+// those of their last step and their observables can still be read.
+__global__ void k_fix_to_float(unsigned long long* __restrict__ fx, float* __restrict__ rho, long long n) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const long long v = (long long)fx[k];
+  rho[k] = (float)((double)v * kInvFix);
+  fx[k] = 0ull;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -330,7 +330,6 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   const int nfft = s_nfft;
   const float* utab = utab_all + sd.utab0 + h;
   const float2* rhok = rhok_all + sd.spec0;
-  float2* gk = gk_all + sd.spec0 * D;
   const float* kd = kd_all + sd.kd0;
   const int ix = (int)(h % g.nxh);
   const long long r = h / g.nxh;
@@ -340,6 +339,12 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   kv[0] = kd[ix];
   kv[1] = kd[g.nx[0] + iy];
   kv[2] = (D == 3) ? kd[g.nx[0] + g.nx[1] + iz] : 0.f;
+  // output: -i k_d P for each channel's potential P, planar per direction (batched C2R input)
+  float2* gk = gk_all + sd.spec0 * D;
+  auto store = [&](int ch, float2 P) {
+#pragma unroll
+    for (int d = 0; d < D; d++) gk[((long long)ch * D + d) * Mh + h] = make_float2(kv[d] * P.y, -kv[d] * P.x);
+  };
   if (NT > 0) {
     constexpr int NA = NT > 0 ? NT : 1;
     float2 rk[NA], phi[NA];
@@ -367,9 +372,7 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
 #pragma unroll
     for (int t = 0; t < NA; t++) {
       if (t >= T) break;
-#pragma unroll
-      for (int d = 0; d < D; d++)  // -i k_d Phi
-        gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
+      store(t, phi[t]);
     }
   } else {  // more types than the specialised kernels cover: same arithmetic, local arrays
     float2 phi[TILD_MAX_TYPES];
@@ -381,16 +384,13 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
       phi[a].x += u * rb.x; phi[a].y += u * rb.y;
       phi[b].x += u * ra.x; phi[b].y += u * ra.y;
     }
-    for (int t = 0; t < T; t++)
-      for (int d = 0; d < D; d++)
-        gk[((long long)t * D + d) * Mh + h] = make_float2(kv[d] * phi[t].y, -kv[d] * phi[t].x);
+    for (int t = 0; t < T; t++) store(t, phi[t]);
   }
   if (C) {
     const float2 rc = rhok[(long long)T * Mh + h];
     const float cm = ctab_all[sd.ctab0 + h];
     const float2 pc = make_float2(cm * rc.x, cm * rc.y);
-#pragma unroll
-    for (int d = 0; d < D; d++) gk[((long long)T * D + d) * Mh + h] = make_float2(kv[d] * pc.y, -kv[d] * pc.x);
+    store(T, pc);
   }
 }
 
@@ -409,12 +409,15 @@ __global__ void k_fieldphase_apply(float* __restrict__ gfield, const float* __re
 
 // Interleave the C2R output [(T+C)][D][M] into one float4 (-dPhi/dx, -dPhi/dy, -dPhi/dz, 0) per
 // grid point and channel, so the gather reads a stencil node with a single 16-byte load.
+// (Writing the float4 field from strided inverse transforms instead was measured slower at 128^3
+// and no faster on small grids.)
 template <int D>
 __global__ void k_interleave(const float* __restrict__ planar_all, float4* __restrict__ g4_all,
                              const int* __restrict__ cta_sys, const int* __restrict__ blk0,
                              const SysDev* __restrict__ sysd) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
+  if (!sd.active) return;  // inactive systems are not gathered
   const long long M = sd.g.M;
   const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
   if (m >= M) return;
@@ -616,20 +619,24 @@ __global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
   if (sysd[s].stop_at >= 0 && step >= sysd[s].stop_at) sysd[s].active = 0;
 }
 
+// Order <= 1 always spreads directly; order >= 2 uses the shared box unless the tuner chose the
+// direct kernel.  The box (spread_cap words, at most 12288 = 48 KB) plus the kernel's static
+// shared memory exceeds the default 48 KB, so the opt-in limit is raised once per device.
 template <int D, int P>
 void launch_spread(tild_ctx* c) {
-  if constexpr (P <= 1) {
+  if (P <= 1 || c->spread_mode == TILD_SPREAD_DIRECT) {
     k_spread_direct<D, P><<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
                                                                    c->rho_fx, c->d_status);
-  } else {
-  const size_t smem = sizeof(int) * (size_t)c->spread_cap;
-  static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
-  if (!(attr_devices >> (c->device & 63) & 1ull)) {
-    cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_devices |= 1ull << (c->device & 63);
-  }
-  k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
-                                                                   c->rho_fx, c->spread_cap, c->d_status);
+  } else if constexpr (P >= 2) {
+    static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
+    if (!(attr_devices >> (c->device & 63) & 1ull)) {
+      cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(int) * 12288));
+      attr_devices |= 1ull << (c->device & 63);
+    }
+    const size_t smem = sizeof(int) * (size_t)c->spread_cap;
+    k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead,
+                                                                     c->d_sys, c->rho_fx, c->spread_cap, c->d_status);
   }
 }
 
@@ -690,15 +697,15 @@ void launch_kmul(tild_ctx* c, bool integ) {
 
 // fork the auxiliary streams off the main stream, and join them back
 int fork(tild_ctx* c) {
-  if (c->aux.empty()) return 0;
+  if (c->lanes == 0) return 0;
   if (tild_check(c, cudaEventRecord(c->ev_fork, c->stream), "fork")) return 1;
-  for (cudaStream_t a : c->aux)
-    if (tild_check(c, cudaStreamWaitEvent(a, c->ev_fork, 0), "fork wait")) return 1;
+  for (int k = 0; k < c->lanes; k++)
+    if (tild_check(c, cudaStreamWaitEvent(c->aux[k], c->ev_fork, 0), "fork wait")) return 1;
   return 0;
 }
 
 int join(tild_ctx* c) {
-  for (size_t k = 0; k < c->aux.size(); k++) {
+  for (int k = 0; k < c->lanes; k++) {
     if (tild_check(c, cudaEventRecord(c->ev_join[k], c->aux[k]), "join")) return 1;
     if (tild_check(c, cudaStreamWaitEvent(c->stream, c->ev_join[k], 0), "join wait")) return 1;
   }
@@ -717,8 +724,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (c->D == 3) dispatch_p_spread<3>(c);
   else dispatch_p_spread<2>(c);
   tild_mark(c, STAGE_ZERO);
-  k_fix_to_float<<<c->n_cta_grid, 256, 0, c->stream>>>(c->rho_fx, c->rho, c->cta_grid, c->cta_grid + c->n_cta_grid,
-                                                      c->d_sys);
+  k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
   c->launches += 2;
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
@@ -758,9 +764,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
   if (integrate) {
     tild_mark(c, STAGE_TAIL);
-    bool any_inactive = c->nsys > 1;  // batches always carry the hold kernel (graphs stay valid)
-    for (const SysHost& h : c->sys) any_inactive |= !h.active;
-    if (any_inactive) {
+    if (tild_needs_hold(c)) {
       k_hold_inactive<<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->pos[c->cur ^ 1], c->cta_bead,
                                                                c->d_sys);
       c->launches++;

@@ -55,6 +55,19 @@ class Config(C.Structure):
                 ("sort_interval", C.c_int32), ("flags", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
+SPREAD_TILED, SPREAD_DIRECT = 0, 1
+
+
+class Tune(C.Structure):
+    _fields_ = [("spread_mode", C.c_int32), ("spread_cap", C.c_int32), ("sort_interval", C.c_int32),
+                ("fft_streams", C.c_int32), ("ms_per_step", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"spread_mode": "tiled" if self.spread_mode == SPREAD_TILED else "direct",
+                "spread_cap_words": self.spread_cap, "sort_interval": self.sort_interval,
+                "fft_streams": self.fft_streams, "ms_per_step": self.ms_per_step}
+
+
 class Obs(C.Structure):
     _fields_ = [("upe", C.c_double), ("ubond", C.c_double), ("uelec", C.c_double), ("ptens", C.c_double * 6),
                 ("bond_vir", C.c_double * 6), ("style_energy", C.c_double * MAX_STYLES),
@@ -112,6 +125,9 @@ def lib() -> C.CDLL:
         "tild_batch_create_slots": ([C.POINTER(Config), ip, i32, i32, C.POINTER(vp)], i32),
         "tild_batch_capacity": ([vp, i32, ip], i32), "tild_batch_load": ([vp, i32, C.POINTER(Config)], i32),
         "tild_batch_set_stop": ([vp, i32, C.c_int64], i32), "tild_batch_get_active": ([vp, i32, ip], i32),
+        "tild_autotune": ([vp, i32, C.POINTER(Tune)], i32), "tild_get_tune": ([vp, C.POINTER(Tune)], i32),
+        "tild_set_tune": ([vp, C.POINTER(Tune)], i32), "tild_batch_autotune": ([vp, i32, C.POINTER(Tune)], i32),
+        "tild_batch_get_tune": ([vp, C.POINTER(Tune)], i32), "tild_batch_set_tune": ([vp, C.POINTER(Tune)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -345,6 +361,20 @@ class Context:
         return cell, cnt, nb, cmax
 
     # -- measurement ---------------------------------------------------------------------
+    def autotune(self, trial_steps: int = 64) -> dict:
+        """Times schedule candidates (tild_autotune) and keeps the fastest; the state is restored."""
+        t = Tune()
+        self._check(lib().tild_autotune(self._h, int(trial_steps), C.byref(t)), "tild_autotune")
+        return t.as_dict()
+
+    def get_tune(self) -> Tune:
+        t = Tune()
+        self._check(lib().tild_get_tune(self._h, C.byref(t)), "tild_get_tune")
+        return t
+
+    def set_tune(self, t: Tune):
+        self._check(lib().tild_set_tune(self._h, C.byref(t)), "tild_set_tune")
+
     def time_steps(self, n: int) -> float:
         ms = C.c_double()
         self._check(lib().tild_time_steps(self._h, int(n), C.byref(ms)), "tild_time_steps")
@@ -462,6 +492,12 @@ class Batch:
         self._check(lib().tild_batch_forces(self._h, i, _ptr(f, C.c_float)), "tild_batch_forces")
         return f
 
+    def evaluate(self):
+        """One force evaluation of every system at its current positions, without a step: the
+        densities, spectra and observables afterwards describe the current state (systems that
+        stopped or were set inactive included, their positions being held)."""
+        self._check(lib().tild_batch_forces(self._h, 0, None), "tild_batch_forces")
+
     def observables(self, i: int) -> dict:
         o = Obs()
         self._check(lib().tild_batch_observables(self._h, i, C.byref(o)), "tild_batch_observables")
@@ -473,6 +509,20 @@ class Batch:
         r = np.empty((nch, int(np.prod(s.nx[:s.dim]))), np.float32)
         self._check(lib().tild_batch_get_density(self._h, i, _ptr(r, C.c_float)), "tild_batch_get_density")
         return r
+
+    def autotune(self, trial_steps: int = 64) -> dict:
+        """Times schedule candidates (tild_batch_autotune) and keeps the fastest; states are restored."""
+        t = Tune()
+        self._check(lib().tild_batch_autotune(self._h, int(trial_steps), C.byref(t)), "tild_batch_autotune")
+        return t.as_dict()
+
+    def get_tune(self) -> Tune:
+        t = Tune()
+        self._check(lib().tild_batch_get_tune(self._h, C.byref(t)), "tild_batch_get_tune")
+        return t
+
+    def set_tune(self, t: Tune):
+        self._check(lib().tild_batch_set_tune(self._h, C.byref(t)), "tild_batch_set_tune")
 
     def time_steps(self, n: int) -> float:
         ms = C.c_double()

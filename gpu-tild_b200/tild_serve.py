@@ -11,7 +11,9 @@ capacity, so its state stays resident in HBM.  The loop
      device-side stop at the job's step count);
   2. advances every active slot by one epoch of `epoch` steps in one stepping call (CUDA graphs,
      one launch per stage for all slots), so jobs admitted at different times overlap on the GPU;
-  3. records each running job's energy (FP64 observables) and accumulates its avg_sk;
+  3. evaluates the densities of every slot at its current positions (one force evaluation without a
+     step; stopped slots hold their last positions) and records each running job's energy (FP64
+     observables) and accumulates its avg_sk, so every record describes the state at its step;
   4. retires the jobs whose slots left the active set on the device (their last step ran inside
      the epoch), returning the energy trace and S(k) and freeing the slot for the queue.
 
@@ -89,7 +91,7 @@ class Server:
     def __init__(self, slots_per_edge: Dict[int, int], capacity_of: Callable[[int], int] = ts.ensemble_capacity,
                  template_of: Callable[[int], tild.System] = ts.ensemble_slot_template, device: int = 0,
                  hbm_budget: float = 80e9, epoch: int = 128, keep_positions: bool = False,
-                 measure_memory: bool = True):
+                 measure_memory: bool = True, tune: bool = False):
         self.device = device
         self.epoch = int(epoch)
         self.keep_positions = keep_positions
@@ -108,6 +110,8 @@ class Server:
         if self.pool_bytes > self.hbm_budget:
             self.batch.close()
             raise MemoryError(f"slot pool needs {self.pool_bytes / 1e9:.1f} GB, budget {self.hbm_budget / 1e9:.1f} GB")
+        # schedule chosen on the full pool (every slot holding its template system)
+        self.schedule = self.batch.autotune(trial_steps=64) if tune else None
         for i in range(len(systems)):
             self.batch.set_active(i, False)
         self.free: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
@@ -176,6 +180,8 @@ class Server:
                 continue
             ts0 = time.perf_counter()
             self.batch.step(self.epoch)
+            # records describe each job's state after the epoch (stopped jobs: their last step)
+            self.batch.evaluate()
             self.stepping_s += time.perf_counter() - ts0
             self.epochs_run += 1
             epoch_no += 1

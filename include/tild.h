@@ -271,6 +271,30 @@ int32_t tild_batch_load(tild_batch* b, int32_t sys, const tild_config* cfg);
 int32_t tild_batch_set_stop(tild_batch* b, int32_t sys, int64_t stop_at);
 int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active);
 
+/* ---- schedule tuning (no reference counterpart) --------------------------------------------- */
+/* Settings that change how, not what, the step computes: densities are fixed-point sums and
+ * every other kernel is per bead or per grid point, so results are bitwise the same under any of
+ * them. */
+enum { TILD_SPREAD_TILED = 0, TILD_SPREAD_DIRECT = 1 };
+typedef struct tild_tune {
+  int32_t spread_mode;    /* order >= 2: shared-memory box per 256 beads (TILED) or 64-bit global atomics (DIRECT) */
+  int32_t spread_cap;     /* shared box of the tiled spread, 32-bit words, 1024..12288 */
+  int32_t sort_interval;  /* steps between spatial sorts; 0 = never (only when the context sorts) */
+  int32_t fft_streams;    /* auxiliary streams the per-grid-shape FFTs are spread over (0..8) */
+  double ms_per_step;     /* tild_autotune: measured step time with these settings */
+} tild_tune;
+int32_t tild_get_tune(tild_ctx* ctx, tild_tune* out);
+int32_t tild_set_tune(tild_ctx* ctx, const tild_tune* t);
+/* Times candidate settings (coordinate descent over spread mode, box size, sort interval and FFT
+ * streams, each trial trial_steps steps after one graph period of warm-up) and keeps the fastest.
+ * The state of every system (positions, x_{n-1}, noise, step counters, activity) is restored
+ * afterwards, so tuning does not advance the simulation.  Not available with TILD_RNG_XORWOW (the
+ * generator states would advance). */
+int32_t tild_autotune(tild_ctx* ctx, int32_t trial_steps, tild_tune* best);
+int32_t tild_batch_autotune(tild_batch* b, int32_t trial_steps, tild_tune* best);
+int32_t tild_batch_get_tune(tild_batch* b, tild_tune* out);
+int32_t tild_batch_set_tune(tild_batch* b, const tild_tune* t);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (code that
  * runs inside another framework's allocator, or after device allocation has been closed): the

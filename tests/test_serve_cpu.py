@@ -49,6 +49,9 @@ class FakeBatch:
                     if self.stop[i] >= 0 and self.stepc[i] >= self.stop[i]:
                         self.act[i] = False
 
+    def evaluate(self):
+        pass
+
     def observables(self, i):
         return {"upe": float(self.stepc[i]) + 0.5 * i}
 

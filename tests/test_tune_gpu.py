@@ -1,0 +1,76 @@
+"""Schedule tuning changes how, not what, a step computes: every setting gives bitwise the same
+trajectory, and tild_autotune leaves the simulation state where it found it."""
+import numpy as np
+import pytest
+
+import tild
+from helpers import small_diblock
+
+pytestmark = pytest.mark.gpu
+
+
+def p3_system():
+    return small_diblock(3, 3, nx=(20, 18, 16), box=(10.0, 9.0, 8.0), n_chains=150, N=10, seed=31)
+
+
+def run(s, tune=None, steps=70):
+    with tild.Context(s) as c:
+        if tune is not None:
+            t = c.get_tune()
+            for k, v in tune.items():
+                setattr(t, k, v)
+            c.set_tune(t)
+        c.step(steps)
+        return c.get_state()
+
+
+@pytest.mark.parametrize("tune", [
+    {"spread_mode": tild.SPREAD_DIRECT},
+    {"spread_cap": 1024},                 # most chunks overflow the box and fall back to global atomics
+    {"sort_interval": 8},
+    {"sort_interval": 32},
+])
+def test_every_setting_gives_the_same_trajectory(tune):
+    s = p3_system()
+    ref = run(s)
+    got = run(s, tune)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+
+
+def test_autotune_restores_state_and_keeps_results():
+    s = p3_system()
+    with tild.Context(s) as c:
+        c.step(20)
+        x0 = c.get_state()
+        best = c.autotune(trial_steps=32)
+        assert best["ms_per_step"] > 0
+        assert c.step_count == 20
+        for a, b in zip(x0, c.get_state()):
+            assert np.array_equal(a, b)
+        c.step(50)
+        got = c.get_state()
+    ref = run(s, steps=70)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+
+
+def test_batch_autotune_streams():
+    systems = [small_diblock(3, 1, nx=(16, 16, 16), box=(8.0, 8.0, 8.0), seed=41),
+               small_diblock(3, 1, nx=(12, 14, 16), box=(6.0, 7.0, 8.0), n_chains=70, seed=42),
+               small_diblock(3, 1, nx=(20, 20, 20), box=(10.0, 10.0, 10.0), n_chains=200, seed=43)]
+    with tild.Batch(systems) as B:
+        before = [B.get_state(i) for i in range(3)]
+        best = B.autotune(trial_steps=32)
+        assert 0 <= best["fft_streams"] <= 8
+        for i in range(3):
+            assert B.step_count(i) == 0
+            for a, b in zip(before[i], B.get_state(i)):
+                assert np.array_equal(a, b)
+        B.step(40)
+        tuned = [B.get_state(i)[0] for i in range(3)]
+    with tild.Batch(systems) as B:
+        B.step(40)
+        plain = [B.get_state(i)[0] for i in range(3)]
+    for a, b in zip(tuned, plain):
+        assert np.array_equal(a, b)
