@@ -43,6 +43,16 @@ FALLBACK_HBM_GBS = 6650.0
 C_SIZEOF_OBS = __import__("ctypes").sizeof(tild.Obs)
 
 
+def nvtx_range(name: str):
+    """An NVTX range around a timed region, so a profiler can select exactly its launches."""
+    try:
+        import torch
+        return torch.cuda.nvtx.range(name)
+    except Exception:
+        import contextlib
+        return contextlib.nullcontext()
+
+
 def ensemble(n: int = 256):
     return [ts.ensemble_member(i) for i in range(n)]
 
@@ -60,7 +70,7 @@ def run_ensemble(args):
     B.step(args.warmup * 32)
     B.sync()
     grp.barrier()
-    with ClockSampler(grp.local) as clk:
+    with ClockSampler(grp.local) as clk, nvtx_range("timed"):
         ms = B.time_steps(args.steps)
     ms = grp.max(ms)
     tot = grp.sum(sum(s.ns for s in local)) * args.steps
@@ -90,6 +100,24 @@ def run_ensemble(args):
         out["serial"] = {"value": serial_value, "unit": "particle-steps/s",
                          "sample": f"{len(sample)} of {args.nsys} systems, each alone for {args.steps} steps"}
         out["batched_over_serial"] = value / serial_value
+        if not args.no_reference_cuda:
+            # the reference's own build, one system per process as it runs them
+            ref_sample = sample[::4]
+            t_ref, ns_ref = 0.0, 0
+            for i in ref_sample:
+                r = reference_cuda(systems[i], "ensemble_member")
+                if r is None or "unavailable" in r:
+                    t_ref = None
+                    break
+                t_ref += r["ms_per_step"] / 1e3
+                ns_ref += systems[i].ns
+            if t_ref:
+                ref_value = ns_ref / t_ref
+                out["reference_cuda_serial"] = {
+                    "value": ref_value, "unit": "particle-steps/s",
+                    "sample": f"{len(ref_sample)} of {args.nsys} systems, each a separate run of the reference build "
+                              "(per-step time from two run lengths)"}
+                out["batched_over_reference_serial"] = value / ref_value
     grp.close()
     if grp.rank == 0:
         print(json.dumps(out))
@@ -279,7 +307,7 @@ def run_ours(args):
     ctx.step(args.warmup)
     ctx.sync()
     grp.barrier()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk, nvtx_range("timed"):
         l0 = ctx.kernel_launches()
         ms = ctx.time_steps(args.steps)
         launches = ctx.kernel_launches() - l0
@@ -370,9 +398,14 @@ def cpu_baseline(s, args, target_s: float = 20.0):
                       f"(oracle/tild_oracle.c, FP64, OpenMP {cores} threads)"}
 
 
-def reference_cuda(s, wname, steps=(20, 120)):
+def reference_cuda(s, wname, steps=None):
     """The reference program built from its own sources (oracle/_ref/gpu-tild) on this GPU:
-    per-step time = difference of wall times of two runs that differ only in max_steps."""
+    per-step time = difference of wall times of two runs that differ only in max_steps.  The
+    longer run is sized (about 3 s of stepping at the reference's C2 rate per bead, at least 100
+    steps) so the difference dominates the run-to-run spread of process start-up."""
+    if steps is None:
+        extra = int(min(20000, max(100, 3.0 / (s.ns * 4e-9))))
+        steps = (20, 20 + extra)
     exe = os.path.join(ROOT, "oracle", "_ref", "gpu-tild")
     if not os.path.exists(exe):
         return None

@@ -901,11 +901,6 @@ int sys_sk_get(tild_ctx* c, int s, int slot, double* sk, int32_t* ncalls) {
   return TILD_OK;
 }
 
-void drop_graphs(tild_ctx* c) {
-  for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
-  c->graphs.clear();
-}
-
 // ---- schedule tuning -------------------------------------------------------------------------
 void get_tune(const tild_ctx* c, tild_tune* t) {
   t->spread_mode = c->spread_mode;
@@ -1293,11 +1288,7 @@ int32_t tild_batch_capacity(tild_batch* b, int32_t sys, int32_t* capacity) {
 int32_t tild_batch_set_stop(tild_batch* b, int32_t sys, int64_t stop_at) {
   if (check_sys(b, sys) || stop_at < -1) return TILD_ERR_BAD_INPUT;
   b->h_sys[sys].stop_at = stop_at;
-  if (stop_at >= 0 && !b->any_stop) {
-    const bool hold_before = tild_needs_hold(b);
-    b->any_stop = true;
-    if (!hold_before) drop_graphs(b);
-  }
+  if (stop_at >= 0) b->any_stop = true;
   return tild_upload_sys(b);
 }
 int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active) {
@@ -1327,9 +1318,7 @@ int32_t tild_batch_set_active(tild_batch* b, int32_t sys, int32_t active) {
   if (check_sys(b, sys)) return TILD_ERR_BAD_INPUT;
   if (active && b->h_sys[sys].stop_at >= 0 && b->sys[sys].step >= b->h_sys[sys].stop_at)
     return set_err(b, TILD_ERR_STATE, "the system is at or past its stop step");
-  const bool hold_before = tild_needs_hold(b);
   b->sys[sys].active = active != 0;
-  if (!hold_before && tild_needs_hold(b)) drop_graphs(b);
   return tild_upload_sys(b);
 }
 int32_t tild_batch_set_step(tild_batch* b, int32_t sys, int64_t step) { return sys_set_step(b, sys, step); }

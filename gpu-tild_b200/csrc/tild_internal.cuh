@@ -360,15 +360,7 @@ int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);
 int tild_assign_lanes(tild_ctx* c, int lanes);
 
-// Whether a step must carry k_hold_inactive (a system may be inactive while others step).
-// Several systems, a device-side stop or an inactive system make it so; captured graphs are
-// dropped when this turns true.
-inline bool tild_needs_hold(const tild_ctx* c) {
-  if (c->nsys > 1 || c->any_stop) return true;
-  for (const SysHost& h : c->sys)
-    if (!h.active) return true;
-  return false;
-}
+
 int tild_table_plans(tild_ctx* c, const Geom& g, int D, cufftHandle* z2d, cufftHandle* d2z);
 void tild_tables_free(tild_ctx* c);
 int tild_stencil_run(tild_ctx* c, int s, int* inds_dev, float* w_dev);

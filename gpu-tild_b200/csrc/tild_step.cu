@@ -470,8 +470,11 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
     int* status) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
-  if (!sd.active) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!sd.active) {
+    if (INTEG) pos_io[i] = pos_in[i];  // inactive systems keep x_n through the buffer rotation
+    return;
+  }
   const float4 p = pos_in[i];
   const int t = tild_type_of(p.w);
   if (t == kPadType) return;
@@ -494,6 +497,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
   const int bid = bead_id[i];
   float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
   if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
+
   float f[3] = {0.f, 0.f, 0.f};
   {
     float W[3][P + 1];
@@ -598,15 +602,6 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
 #pragma unroll
     for (int d = 0; d < D; d++) noise[3 * (long long)i + d] = on[d];
   }
-}
-
-// inactive systems keep their slots: copy x_n into the rotated buffer so their state survives
-__global__ void k_hold_inactive(const float4* __restrict__ pos_in, float4* __restrict__ pos_io,
-                                const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd) {
-  const SysDev& sd = sysd[cta_sys[blockIdx.x]];
-  if (sd.active) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  pos_io[i] = pos_in[i];
 }
 
 // step counters advance on the device; a system whose counter reaches its stop step leaves the
@@ -764,11 +759,6 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
   if (integrate) {
     tild_mark(c, STAGE_TAIL);
-    if (tild_needs_hold(c)) {
-      k_hold_inactive<<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->pos[c->cur ^ 1], c->cta_bead,
-                                                               c->d_sys);
-      c->launches++;
-    }
     k_advance_steps<<<nblk(c->nsys, 128), 128, 0, c->stream>>>(c->d_sys, c->nsys);
     c->launches++;
     c->cur ^= 1;
