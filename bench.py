@@ -43,6 +43,11 @@ FALLBACK_HBM_GBS = 6650.0
 C_SIZEOF_OBS = __import__("ctypes").sizeof(tild.Obs)
 
 
+def graph_period(tune) -> int:
+    """Steps per captured CUDA graph: two sort periods (32 when the sort is off)."""
+    return 2 * tune.sort_interval if tune.sort_interval > 0 else 32
+
+
 def nvtx_range(name: str):
     """An NVTX range around a timed region, so a profiler can select exactly its launches."""
     try:
@@ -67,7 +72,9 @@ def run_ensemble(args):
     local = [systems[i] for i in mine]
     B = tild.Batch(local, device=grp.local)
     schedule = None if args.no_tune else B.autotune(trial_steps=64)
-    B.step(args.warmup * 32)
+    period = graph_period(B.get_tune())
+    args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
+    B.step(-(-args.warmup * 32 // period) * period)
     B.sync()
     grp.barrier()
     with ClockSampler(grp.local) as clk, nvtx_range("timed"):
@@ -304,6 +311,8 @@ def run_ours(args):
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
     schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
+    period = graph_period(ctx.get_tune())
+    args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
     ctx.step(args.warmup)
     ctx.sync()
     grp.barrier()

@@ -325,6 +325,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   c->h_sys.assign(nsys, SysDev());
   memset(c->h_sys.data(), 0, sizeof(SysDev) * nsys);
   c->sort_interval = cfgs[0].sort_interval == 0 ? 16 : (cfgs[0].sort_interval < 0 ? 0 : cfgs[0].sort_interval);
+  c->sort_brick = tild_brick_candidates(cfgs[0].dim == 2 ? 2 : 3)[0];
   c->steps_since_sort = c->sort_interval;
   c->spread_cap = 12288;
   long long slots = 0, beads = 0, utab = 0, virk = 0, ctab = 0, kd = 0, fr = 0;
@@ -907,18 +908,34 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
   t->spread_cap = c->spread_cap;
   t->sort_interval = c->sort_interval;
   t->fft_streams = c->lanes;
+  t->gather_mode = c->gather_mode;
+  t->gather_cap = c->gather_cap;
+  t->sort_brick = c->sort_brick;
   t->ms_per_step = 0.0;
 }
 
 int set_tune(tild_ctx* c, const tild_tune* t) {
   if (!t || (t->spread_mode != TILD_SPREAD_TILED && t->spread_mode != TILD_SPREAD_DIRECT) || t->spread_cap < 1024 ||
-      t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8)
+      t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
+      (t->gather_mode != TILD_GATHER_DIRECT && t->gather_mode != TILD_GATHER_BOX) || t->gather_cap < 1024 ||
+      t->gather_cap > 3072)
     return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
   if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
+  {
+    const auto cand = tild_brick_candidates(c->D);
+    if (std::find(cand.begin(), cand.end(), (int)t->sort_brick) == cand.end())
+      return set_err(c, TILD_ERR_BAD_INPUT, "sort_brick is not one of the supported brick shapes");
+  }
   cudaSetDevice(c->device);
   if (tild_check(c, cudaStreamSynchronize(c->stream), "sync before tune")) return TILD_ERR_CUDA;
   c->spread_mode = t->spread_mode;
   c->spread_cap = t->spread_cap;
+  c->gather_mode = t->gather_mode;
+  c->gather_cap = t->gather_cap;
+  if (t->sort_brick != c->sort_brick) {
+    c->sort_brick = t->sort_brick;
+    c->steps_since_sort = c->sort_interval;  // re-sort with the new keys at the next step
+  }
   if (t->sort_interval != c->sort_interval) {
     c->sort_interval = t->sort_interval;
     c->steps_since_sort = c->sort_interval;
@@ -989,7 +1006,24 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
         t.spread_cap = cap;
         if (cap != cur.spread_cap) consider(t);
       }
+    for (int mode : {TILD_GATHER_DIRECT, TILD_GATHER_BOX}) {
+      tild_tune t = cur;
+      t.gather_mode = mode;
+      if (mode != cur.gather_mode) consider(t);
+    }
+    if (cur.gather_mode == TILD_GATHER_BOX)
+      for (int cap : {1536, 2048, 3072}) {
+        tild_tune t = cur;
+        t.gather_cap = cap;
+        if (cap != cur.gather_cap) consider(t);
+      }
   }
+  if (c->sort_temp)
+    for (int brick : tild_brick_candidates(c->D)) {
+      tild_tune t = cur;
+      t.sort_brick = brick;
+      if (brick != cur.sort_brick) consider(t);
+    }
   if (c->sort_temp)
     for (int si : {8, 16, 32}) {
       tild_tune t = cur;

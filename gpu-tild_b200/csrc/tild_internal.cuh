@@ -119,6 +119,9 @@ struct tild_ctx {
   int lanes = 0;                         // auxiliary streams in use (tild_assign_lanes)
   // tunables (tild_autotune): spread kernel for order >= 2 and its shared box, in 32-bit words
   int spread_mode = TILD_SPREAD_TILED;
+  int gather_mode = TILD_GATHER_DIRECT;  // order >= 2: stencil reads from global memory or a shared box
+  int gather_cap = 3072;                 // float4 nodes of the gather box, 1024..3072
+  int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
   int D = 3, P = 1;
   int nsys = 1;
   std::vector<SysHost> sys;
@@ -359,6 +362,13 @@ int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);
 int tild_assign_lanes(tild_ctx* c, int lanes);
+
+// Brick shapes of the spatial sort the tuner chooses from (log2 edges x | y<<4 | z<<8, bit 12 =
+// Morton order of the bricks); the first is the default.
+inline std::vector<int> tild_brick_candidates(int D) {
+  if (D == 3) return {0x222, 0x1222, 0x1113, 0x1123};
+  return {0x033, 0x1033, 0x1014};
+}
 
 
 int tild_table_plans(tild_ctx* c, const Geom& g, int D, cufftHandle* z2d, cufftHandle* d2z);

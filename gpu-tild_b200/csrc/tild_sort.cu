@@ -21,8 +21,11 @@ __device__ __forceinline__ int ilog2c(int v) {
   return s;
 }
 
+// Sort key of a slot: the system in the high bits, then the brick of its grid cell, then the cell
+// inside the brick (x fastest).  `brick` packs log2 of the brick edges (bits 0-3 x, 4-7 y, 8-11 z,
+// each capped by the grid) and bit 12 orders bricks along a Morton curve instead of x-fastest.
 __global__ void k_sort_keys(const float4* __restrict__ pos, const int* __restrict__ cta_sys,
-                            const SysDev* __restrict__ sysd, int D, int cell_bits, unsigned* __restrict__ keys,
+                            const SysDev* __restrict__ sysd, int D, int cell_bits, int brick, unsigned* __restrict__ keys,
                             int* __restrict__ vals) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   const int sys = cta_sys[blockIdx.x];
@@ -32,19 +35,29 @@ __global__ void k_sort_keys(const float4* __restrict__ pos, const int* __restric
   unsigned cell = pad_code;
   if (tild_type_of(p.w) != kPadType) {
     const float xs[3] = {p.x, p.y, p.z};
-    int c[3] = {0, 0, 0}, sh[3] = {0, 0, 0}, nb[3] = {1, 1, 1};
+    int c[3] = {0, 0, 0}, sh[3] = {0, 0, 0}, nb[3] = {1, 1, 1}, bb[3] = {0, 0, 0};
     for (int d = 0; d < D; d++) {
       int v = isfinite(xs[d]) ? (int)(xs[d] / g.dx[d]) : 0;
       c[d] = min(max(v, 0), g.nx[d] - 1);
-      const int edge = min(D == 3 ? 4 : 8, 1 << ilog2c(g.nx[d]));
-      sh[d] = ilog2c(edge);
-      nb[d] = (g.nx[d] + edge - 1) / edge;
+      sh[d] = min((brick >> (4 * d)) & 15, ilog2c(g.nx[d]));
+      nb[d] = (g.nx[d] + (1 << sh[d]) - 1) >> sh[d];
+      bb[d] = ilog2c(nb[d]);
     }
-    const unsigned brick = ((unsigned)(c[2] >> sh[2]) * nb[1] + (unsigned)(c[1] >> sh[1])) * nb[0] + (c[0] >> sh[0]);
+    unsigned bidx;
+    if (brick >> 12 & 1) {  // Morton order of the bricks: bits interleaved x, y, z
+      const int nmax = max(bb[0], max(bb[1], bb[2]));
+      bidx = 0;
+      int o = 0;
+      for (int b = 0; b < nmax; b++)
+        for (int d = 0; d < 3; d++)
+          if (b < bb[d]) bidx |= (((unsigned)(c[d] >> sh[d]) >> b) & 1u) << o++;
+    } else {
+      bidx = ((unsigned)(c[2] >> sh[2]) * nb[1] + (unsigned)(c[1] >> sh[1])) * nb[0] + (c[0] >> sh[0]);
+    }
     const unsigned local = ((((unsigned)c[2] & ((1u << sh[2]) - 1)) << sh[1]) | ((unsigned)c[1] & ((1u << sh[1]) - 1)))
                                << sh[0] |
                            ((unsigned)c[0] & ((1u << sh[0]) - 1));
-    cell = (brick << (sh[0] + sh[1] + sh[2])) | local;
+    cell = (bidx << (sh[0] + sh[1] + sh[2])) | local;
   }
   keys[slot] = ((unsigned)sys << cell_bits) | cell;
   vals[slot] = slot;
@@ -106,19 +119,23 @@ int tild_sort_alloc(tild_ctx* c) {
     c->err = "device allocation failed: sort buffers";
     return TILD_ERR_OOM;
   }
-  // cell code bits: bricks of 4^3 cells (8^2 in 2D) of the largest system, plus the padding code
+  // cell code bits: enough for every brick shape the tuner may choose, for the largest system,
+  // with the all-ones code left for padding slots
   int cell_bits = 1;
-  for (const SysHost& h : c->sys) {
-    int bits = 0;
-    long long nbricks = 1;
-    for (int d = 0; d < c->D; d++) {
-      const int edge = std::min(c->D == 3 ? 4 : 8, 1 << log2_ceil(h.g.nx[d]));
-      bits += log2_ceil(edge);
-      nbricks *= (h.g.nx[d] + edge - 1) / edge;
+  for (const SysHost& h : c->sys)
+    for (int brick : tild_brick_candidates(c->D)) {
+      int local = 0, bbits = 0;
+      long long nbricks = 1;
+      for (int d = 0; d < c->D; d++) {
+        const int sh = std::min((brick >> (4 * d)) & 15, log2_ceil(h.g.nx[d]));
+        const long long nb = (h.g.nx[d] + (1 << sh) - 1) >> sh;
+        local += sh;
+        nbricks *= nb;
+        bbits += log2_ceil(nb);
+      }
+      const int bits = local + ((brick >> 12 & 1) ? bbits + 1 : log2_ceil(nbricks + 1));
+      cell_bits = std::max(cell_bits, bits);
     }
-    bits += log2_ceil(nbricks + 1);
-    cell_bits = std::max(cell_bits, bits);
-  }
   const int sys_bits = log2_ceil(c->nsys);
   if (cell_bits + sys_bits > 32) {
     c->err = "spatial sort keys need more than 32 bits (too many systems or too large a grid)";
@@ -152,7 +169,7 @@ int tild_sort_beads(tild_ctx* c) {
   const unsigned nb = nblk(n, kTile);
   cudaStream_t st = c->stream;
   k_sort_keys<<<c->n_cta_bead, kTile, 0, st>>>(c->pos[c->cur], c->cta_bead, c->d_sys, c->D, c->sort_cell_bits,
-                                               c->sort_keys, c->sort_vals);
+                                               c->sort_brick, c->sort_keys, c->sort_vals);
   c->launches++;
   size_t tb = c->sort_temp_bytes;
   if (cub::DeviceRadixSort::SortPairs(c->sort_temp, tb, c->sort_keys, c->sort_keys_alt, c->sort_vals, c->sort_perm, n,

@@ -23,6 +23,7 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 constexpr double kInvFix = 1.0 / 4294967296.0;  // the global accumulator holds 2^32 per unit
 constexpr int kMaxRows = 1024;                  // (y, z) rows of a shared-memory spread box
+constexpr int kGatherBoxMax = 3072;             // float4 nodes of the gather's shared box (48 KB)
 
 __device__ __forceinline__ int fold_rel(int r, int N) {
   r %= N;
@@ -461,64 +462,15 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ F, const floa
     }
 }
 
-template <int D, int P, bool INTEG, bool XW>
-__global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather(
-    const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
-    const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
-    const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
-    const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
-    int* status) {
-  const int s = cta_sys[blockIdx.x];
-  const SysDev& sd = sysd[s];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!sd.active) {
-    if (INTEG) pos_io[i] = pos_in[i];  // inactive systems keep x_n through the buffer rotation
-    return;
-  }
-  const float4 p = pos_in[i];
-  const int t = tild_type_of(p.w);
-  if (t == kPadType) return;
-  float x[3] = {p.x, p.y, p.z};
-  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
-    atomicOr(status, ST_NONFINITE_POS);
-    return;  // left in place; the host reports TILD_ERR_NAN
-  }
-  const Geom& g = sd.g;
-  const long long M = g.M;
-  const int T = sd.T, C = sd.C;
-  const float4* g4 = g4_all + sd.grid0;
-  // loads that do not depend on the stencil are issued before it, so their latency overlaps
-  const int info = bond_info[i];
-  const int nb = info & 3;
-  float4 pj[3];
-#pragma unroll
-  for (int bb = 0; bb < 3; bb++)
-    if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
-  const int bid = bead_id[i];
-  float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
-
-  float f[3] = {0.f, 0.f, 0.f};
-  {
-    float W[3][P + 1];
-    int idx[3][P + 1];
-#pragma unroll
-    for (int d = 0; d < D; d++) {
-      const int b = axis_base<P>(x[d], g.dx[d], W[d]);
-#pragma unroll
-      for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
-    }
-    if (C) {
-      const float q = charge[i];
-      if (q != 0.f) {
-        float e[3] = {0.f, 0.f, 0.f};
-        gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
-#pragma unroll
-        for (int d = 0; d < D; d++) f[d] += e[d] * q;
-      }
-    }
-    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
-  }
+// Bonds, the force output and the integrators of one bead: d_bonds (device_bonds.cu:4-60) and
+// Integrate_2 (integrator.cu:24-39) over the integrators in input order.  Shared by both gathers.
+template <int D, bool INTEG, bool XW>
+__device__ __forceinline__ void bead_epilogue(int i, const float4& p, int t, float (&x)[3], float (&f)[3],
+                                              const SysDev& sd, const Geom& g, int info, int nb,
+                                              const float4 (&pj)[3], int bid, const float4& po,
+                                              float* __restrict__ noise, float4* __restrict__ pos_io,
+                                              float* __restrict__ f_out, int f_sys, int s,
+                                              curandStateXORWOW_t* __restrict__ xw) {
   // bonds
 #pragma unroll
   for (int bb = 0; bb < 3; bb++) {
@@ -604,6 +556,222 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather
   }
 }
 
+template <int D, int P, bool INTEG, bool XW>
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather(
+    const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
+    const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
+    const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
+    const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
+    int* status) {
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!sd.active) {
+    if (INTEG) pos_io[i] = pos_in[i];  // inactive systems keep x_n through the buffer rotation
+    return;
+  }
+  const float4 p = pos_in[i];
+  const int t = tild_type_of(p.w);
+  if (t == kPadType) return;
+  float x[3] = {p.x, p.y, p.z};
+  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+    atomicOr(status, ST_NONFINITE_POS);
+    return;  // left in place; the host reports TILD_ERR_NAN
+  }
+  const Geom& g = sd.g;
+  const long long M = g.M;
+  const int T = sd.T, C = sd.C;
+  const float4* g4 = g4_all + sd.grid0;
+  // loads that do not depend on the stencil are issued before it, so their latency overlaps
+  const int info = bond_info[i];
+  const int nb = info & 3;
+  float4 pj[3];
+#pragma unroll
+  for (int bb = 0; bb < 3; bb++)
+    if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
+  const int bid = bead_id[i];
+  float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
+
+  float f[3] = {0.f, 0.f, 0.f};
+  {
+    float W[3][P + 1];
+    int idx[3][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const int b = axis_base<P>(x[d], g.dx[d], W[d]);
+#pragma unroll
+      for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
+    }
+    if (C) {
+      const float q = charge[i];
+      if (q != 0.f) {
+        float e[3] = {0.f, 0.f, 0.f};
+        gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
+#pragma unroll
+        for (int d = 0; d < D; d++) f[d] += e[d] * q;
+      }
+    }
+    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
+  }
+  bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
+}
+
+// The same stencil sums read from a shared-memory box: the CTA's 256 slots (spatially sorted, so
+// a few bricks of cells) need a box of roughly 11x11x7 nodes per channel at order 3.  The box is
+// loaded once with coalesced rows, then every bead reads its (P+1)^D nodes from shared memory in
+// the gather4 order, so forces are bitwise those of k_gather.  A chunk whose box does not fit
+// reads global memory like k_gather.
+template <int D, int P>
+__device__ __forceinline__ void box_gather4(const float4* __restrict__ B, const float (&W)[3][P + 1],
+                                            const int (&lb)[3], int ex, int exy, float (&acc)[3]) {
+#pragma unroll
+  for (int ix = 0; ix <= P; ix++)
+#pragma unroll
+    for (int iy = 0; iy <= P; iy++) {
+      const float wxy = W[0][ix] * W[1][iy];
+      const int row = (lb[1] + iy) * ex + lb[0] + ix;
+      if (D == 3) {
+#pragma unroll
+        for (int iz = 0; iz <= P; iz++) {
+          const float4 v = B[row + (lb[2] + iz) * exy];
+          const float w = wxy * W[2][iz];
+          acc[0] += v.x * w;
+          acc[1] += v.y * w;
+          acc[2] += v.z * w;
+        }
+      } else {
+        const float4 v = B[row];
+        acc[0] += v.x * wxy;
+        acc[1] += v.y * wxy;
+      }
+    }
+}
+
+template <int D, int P, bool INTEG, bool XW>
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
+    const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
+    const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
+    const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
+    const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
+    int box_cap, int* status) {
+  extern __shared__ float4 sbox[];
+  __shared__ int s_g0[3], s_min[3], s_max[3];
+  __shared__ int s_row[kMaxRows];
+  const int s = cta_sys[blockIdx.x];
+  const SysDev& sd = sysd[s];
+  const int i0 = blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
+  if (!sd.active) {  // one system per CTA: every thread leaves here together
+    if (INTEG) pos_io[i] = pos_in[i];
+    return;
+  }
+  const Geom g = sd.g;
+  chunk_origin<D, P>(pos_in, i0, g, s_g0, s_min, s_max);
+  const float4 p = pos_in[i];
+  const int t = tild_type_of(p.w);
+  float x[3] = {p.x, p.y, p.z};
+  bool ok = t != kPadType;
+  if (ok && !(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+    atomicOr(status, ST_NONFINITE_POS);
+    ok = false;  // left in place; the host reports TILD_ERR_NAN
+  }
+  float W[3][P + 1];
+  int rel[3] = {0, 0, 0}, base[3] = {0, 0, 0};
+  if (ok) {
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      base[d] = axis_base<P>(x[d], g.dx[d], W[d]);
+      if (base[d] < -g.nx[d] || base[d] + P >= 2 * g.nx[d]) atomicOr(status, ST_INDEX_RANGE);
+      rel[d] = fold_rel(base[d] - s_g0[d], g.nx[d]);
+    }
+  }
+  int info = 0, nb = 0, bid = 0;
+  float4 pj[3];
+  float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (ok) {
+    info = bond_info[i];
+    nb = info & 3;
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++)
+      if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
+    bid = bead_id[i];
+    if (INTEG) po = pos_io[i];
+  }
+  int mn[3], ext[3];
+  long long vol;
+  if (!chunk_box<D, P>(ok, rel, s_min, s_max, mn, ext, vol)) return;
+  const long long M = g.M;
+  const int T = sd.T, C = sd.C, nch = T + C;
+  const float4* g4 = g4_all + sd.grid0;
+  const float q = (C && ok) ? charge[i] : 0.f;
+  float f[3] = {0.f, 0.f, 0.f};
+  const int ex = ext[0], ey = ext[1], ez = ext[2];
+  if (vol * nch <= box_cap && ex <= 64 && ey * ez <= kMaxRows) {
+    // row offsets of the box in the periodic grid, then the rows themselves, lanes along x
+    const int rows = ey * ez;
+    for (int yz = threadIdx.x; yz < rows; yz += blockDim.x) {
+      const int ly = yz % ey, lz = yz / ey;
+      s_row[yz] = (int)((long long)g.nx[0] * (pmod(s_g0[1] + mn[1] + ly, g.nx[1]) +
+                                              (long long)g.nx[1] * (D == 3 ? pmod(s_g0[2] + mn[2] + lz, g.nx[2]) : 0)));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int lpr = ex < 32 ? ex : 32;           // lanes per row
+    const int rpi = 32 / lpr;                    // rows per warp iteration
+    const int my_r = lane / lpr, my_x = lane - my_r * lpr;
+    const int bx = pmod(s_g0[0] + mn[0], g.nx[0]);
+    int xo[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      int xg = bx + my_x + 32 * k;
+      if (xg >= g.nx[0]) xg -= g.nx[0];
+      if (xg >= g.nx[0]) xg %= g.nx[0];
+      xo[k] = xg;
+    }
+    const int nrows = rows * nch;
+    if (my_r < rpi)
+      for (int R = warp * rpi + my_r; R < nrows; R += nwarps * rpi) {
+        const int ch = R / rows, yz = R - ch * rows;
+        const float4* src = g4 + (long long)ch * M + s_row[yz];
+        float4* dst = sbox + (long long)ch * vol + (long long)yz * ex;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int lx = my_x + 32 * k;
+          if (lx < ex) dst[lx] = __ldg(src + xo[k]);
+        }
+      }
+    __syncthreads();
+    if (ok) {
+      int lb[3] = {0, 0, 0};
+#pragma unroll
+      for (int d = 0; d < D; d++) lb[d] = rel[d] - mn[d];
+      if (C && q != 0.f) {
+        float e[3] = {0.f, 0.f, 0.f};
+        box_gather4<D, P>(sbox + (long long)T * vol, W, lb, ex, ex * ey, e);
+#pragma unroll
+        for (int d = 0; d < D; d++) f[d] += e[d] * q;
+      }
+      box_gather4<D, P>(sbox + (long long)t * vol, W, lb, ex, ex * ey, f);
+    }
+  } else if (ok) {
+    int idx[3][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++)
+#pragma unroll
+      for (int a = 0; a <= P; a++) idx[d][a] = pmod(base[d] + a, g.nx[d]);
+    if (C && q != 0.f) {
+      float e[3] = {0.f, 0.f, 0.f};
+      gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
+#pragma unroll
+      for (int d = 0; d < D; d++) f[d] += e[d] * q;
+    }
+    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
+  }
+  if (!ok) return;
+  bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
+}
+
 // step counters advance on the device; a system whose counter reaches its stop step leaves the
 // active set here, so the next launches skip it without the host in the loop
 __global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
@@ -637,6 +805,18 @@ void launch_spread(tild_ctx* c) {
 
 template <int D, int P, bool I, bool X>
 void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
+  if (P >= 2 && c->gather_mode == TILD_GATHER_BOX) {
+    static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
+    if (!(attr_devices >> (c->device & 63) & 1ull)) {
+      cudaFuncSetAttribute(k_gather_box<D, P, I, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(float4) * kGatherBoxMax));
+      attr_devices |= 1ull << (c->device & 63);
+    }
+    k_gather_box<D, P, I, X><<<c->n_cta_bead, kTile, sizeof(float4) * (size_t)c->gather_cap, c->stream>>>(
+        c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
+        c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->gather_cap, c->d_status);
+    return;
+  }
   k_gather<D, P, I, X><<<c->n_cta_bead, kTile, 0, c->stream>>>(
       c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
       c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->d_status);

@@ -56,16 +56,20 @@ class Config(C.Structure):
 
 
 SPREAD_TILED, SPREAD_DIRECT = 0, 1
+GATHER_DIRECT, GATHER_BOX = 0, 1
 
 
 class Tune(C.Structure):
     _fields_ = [("spread_mode", C.c_int32), ("spread_cap", C.c_int32), ("sort_interval", C.c_int32),
-                ("fft_streams", C.c_int32), ("ms_per_step", C.c_double)]
+                ("fft_streams", C.c_int32), ("gather_mode", C.c_int32), ("gather_cap", C.c_int32),
+                ("sort_brick", C.c_int32), ("ms_per_step", C.c_double)]
 
     def as_dict(self) -> dict:
         return {"spread_mode": "tiled" if self.spread_mode == SPREAD_TILED else "direct",
                 "spread_cap_words": self.spread_cap, "sort_interval": self.sort_interval,
-                "fft_streams": self.fft_streams, "ms_per_step": self.ms_per_step}
+                "fft_streams": self.fft_streams, "gather_mode": "box" if self.gather_mode == GATHER_BOX else "direct",
+                "gather_cap_nodes": self.gather_cap, "sort_brick": hex(self.sort_brick),
+                "ms_per_step": self.ms_per_step}
 
 
 class Obs(C.Structure):

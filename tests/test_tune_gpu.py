@@ -29,6 +29,11 @@ def run(s, tune=None, steps=70):
     {"spread_cap": 1024},                 # most chunks overflow the box and fall back to global atomics
     {"sort_interval": 8},
     {"sort_interval": 32},
+    {"sort_brick": 0x1222},
+    {"sort_brick": 0x1113},
+    {"sort_brick": 0x1123, "sort_interval": 8},
+    {"gather_mode": tild.GATHER_BOX},
+    {"gather_mode": tild.GATHER_BOX, "gather_cap": 1024},   # most chunks fall back to global reads
 ])
 def test_every_setting_gives_the_same_trajectory(tune):
     s = p3_system()
