@@ -316,6 +316,8 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   }
   c->device = device;
   if (tild_check(c, cudaSetDevice(device), "cudaSetDevice")) return TILD_ERR_CUDA;
+  if (tild_check(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "device attribute"))
+    return TILD_ERR_CUDA;
   if (tild_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) return TILD_ERR_CUDA;
   c->D = cfgs[0].dim;
   c->P = cfgs[0].pmeorder;
@@ -917,7 +919,7 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
 int set_tune(tild_ctx* c, const tild_tune* t) {
   if (!t || (t->spread_mode != TILD_SPREAD_TILED && t->spread_mode != TILD_SPREAD_DIRECT) || t->spread_cap < 1024 ||
       t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
-      (t->gather_mode != TILD_GATHER_DIRECT && t->gather_mode != TILD_GATHER_BOX) || t->gather_cap < 1024 ||
+      t->gather_mode < TILD_GATHER_DIRECT || t->gather_mode > TILD_GATHER_BOX || t->gather_cap < 1024 ||
       t->gather_cap > 3072)
     return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
   if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
@@ -1011,7 +1013,7 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
       t.gather_mode = mode;
       if (mode != cur.gather_mode) consider(t);
     }
-    if (cur.gather_mode == TILD_GATHER_BOX)
+    if (cur.gather_mode != TILD_GATHER_DIRECT)
       for (int cap : {1536, 2048, 3072}) {
         tild_tune t = cur;
         t.gather_cap = cap;

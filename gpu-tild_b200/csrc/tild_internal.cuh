@@ -111,6 +111,7 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
 
 struct tild_ctx {
   int device = 0;
+  int num_sms = 148;
   cudaStream_t stream = nullptr;
   // auxiliary streams: the FFTs of different grid shapes run concurrently (fork/join by events)
   std::vector<cudaStream_t> aux;
@@ -119,8 +120,8 @@ struct tild_ctx {
   int lanes = 0;                         // auxiliary streams in use (tild_assign_lanes)
   // tunables (tild_autotune): spread kernel for order >= 2 and its shared box, in 32-bit words
   int spread_mode = TILD_SPREAD_TILED;
-  int gather_mode = TILD_GATHER_DIRECT;  // order >= 2: stencil reads from global memory or a shared box
-  int gather_cap = 3072;                 // float4 nodes of the gather box, 1024..3072
+  int gather_mode = TILD_GATHER_DIRECT;  // order >= 2: stencil reads from global memory or shared boxes
+  int gather_cap = 2048;                 // float4 nodes of a gather box buffer, 1024..3072
   int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
   int D = 3, P = 1;
   int nsys = 1;

@@ -67,7 +67,7 @@ class Tune(C.Structure):
     def as_dict(self) -> dict:
         return {"spread_mode": "tiled" if self.spread_mode == SPREAD_TILED else "direct",
                 "spread_cap_words": self.spread_cap, "sort_interval": self.sort_interval,
-                "fft_streams": self.fft_streams, "gather_mode": "box" if self.gather_mode == GATHER_BOX else "direct",
+                "fft_streams": self.fft_streams, "gather_mode": ("direct", "box")[self.gather_mode],
                 "gather_cap_nodes": self.gather_cap, "sort_brick": hex(self.sort_brick),
                 "ms_per_step": self.ms_per_step}
 

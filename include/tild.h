@@ -282,7 +282,8 @@ typedef struct tild_tune {
   int32_t spread_cap;     /* shared box of the tiled spread, 32-bit words, 1024..12288 */
   int32_t sort_interval;  /* steps between spatial sorts; 0 = never (only when the context sorts) */
   int32_t fft_streams;    /* auxiliary streams the per-grid-shape FFTs are spread over (0..8) */
-  int32_t gather_mode;    /* order >= 2: stencil nodes read from global memory (DIRECT) or a shared box (BOX) */
+  int32_t gather_mode;    /* order >= 2: stencil nodes read from global memory (DIRECT) or from a shared
+                             box each CTA stages first (BOX) */
   int32_t gather_cap;     /* shared box of the box gather, float4 nodes, 1024..3072 */
   int32_t sort_brick;     /* sort key bricks: log2 edges x | y<<4 | z<<8, bit 12 = Morton order of the
                              bricks; 3D 0x222 (default), 0x1222, 0x1113, 0x1123; 2D 0x033 (default),
