@@ -93,6 +93,13 @@ void free_all(tild_ctx* c) {
     for (int i = 0; i < TILD_MAX_COMPUTES; i++)
       if (h.sk[i]) cudaFree(h.sk[i]);
   tild_tables_free(c);
+  for (auto& sl : c->snaps) {
+    if (sl.dx) cudaFree(sl.dx);
+    if (sl.drho) cudaFree(sl.drho);
+    if (sl.captured) cudaEventDestroy(sl.captured);
+    if (sl.done) cudaEventDestroy(sl.done);
+  }
+  if (c->snap_stream) cudaStreamDestroy(c->snap_stream);
   for (Bucket& b : c->buckets)
     if (b.planned) {
       cufftDestroy(b.r2c);
@@ -1061,6 +1068,82 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
   return TILD_OK;
 }
 
+// ---- asynchronous snapshots ------------------------------------------------------------------
+int snap_setup(tild_ctx* c) {
+  if (c->snap_stream) return TILD_OK;
+  size_t nx = 1, nr = 1;
+  for (const SysHost& h : c->sys) {
+    nx = std::max(nx, (size_t)h.cap * h.D);
+    nr = std::max(nr, (size_t)((h.T + h.C) * h.g.M));
+  }
+  if (tild_check(c, cudaStreamCreateWithFlags(&c->snap_stream, cudaStreamNonBlocking), "snapshot stream"))
+    return TILD_ERR_CUDA;
+  for (auto& sl : c->snaps) {
+    if (tild_check(c, cudaMalloc(&sl.dx, nx * sizeof(float)), "alloc snapshot") ||
+        tild_check(c, cudaMalloc(&sl.drho, nr * sizeof(float)), "alloc snapshot"))
+      return TILD_ERR_OOM;
+    if (tild_check(c, cudaEventCreateWithFlags(&sl.captured, cudaEventDisableTiming), "snapshot event") ||
+        tild_check(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "snapshot event"))
+      return TILD_ERR_CUDA;
+  }
+  c->snap_x_floats = nx;
+  c->snap_rho_floats = nr;
+  return TILD_OK;
+}
+
+int sys_snapshot_async(tild_ctx* c, int s, float* x, float* rho, int64_t* ticket) {
+  if (check_sys(c, s) || (!x && !rho)) return TILD_ERR_BAD_INPUT;
+  SysHost& h = c->sys[s];
+  if (x && !h.state_set) return set_err(c, TILD_ERR_STATE, "no state");
+  if (rho && !h.have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
+  cudaSetDevice(c->device);
+  int rc = snap_setup(c);
+  if (rc) return rc;
+  const long long t = c->snap_next;
+  auto& sl = c->snaps[t % TILD_SNAPSHOT_SLOTS];
+  // the slot's previous copy must have left its device buffers before they are overwritten
+  if (sl.ticket.load() >= 0 && tild_check(c, cudaEventSynchronize(sl.done), "snapshot slot")) return TILD_ERR_CUDA;
+  const size_t n = (size_t)h.ns * h.D;
+  const size_t nr = (size_t)(h.T + h.C) * h.g.M;
+  if (x) {
+    k_unpack_pos<<<nblk(h.ns_pad, 256), 256, 0, c->stream>>>(c->pos[c->cur] + h.slot0, c->bead_id + h.slot0,
+                                                             h.ns_pad, h.D, sl.dx);
+    c->launches++;
+  }
+  if (rho && tild_check(c, cudaMemcpyAsync(sl.drho, c->rho + h.grid0, nr * sizeof(float), cudaMemcpyDeviceToDevice,
+                                           c->stream), "snapshot rho"))
+    return TILD_ERR_CUDA;
+  if (tild_check(c, cudaEventRecord(sl.captured, c->stream), "snapshot event") ||
+      tild_check(c, cudaStreamWaitEvent(c->snap_stream, sl.captured, 0), "snapshot wait"))
+    return TILD_ERR_CUDA;
+  if ((x && tild_check(c, cudaMemcpyAsync(x, sl.dx, n * sizeof(float), cudaMemcpyDeviceToHost, c->snap_stream),
+                       "snapshot x")) ||
+      (rho && tild_check(c, cudaMemcpyAsync(rho, sl.drho, nr * sizeof(float), cudaMemcpyDeviceToHost, c->snap_stream),
+                         "snapshot rho")))
+    return TILD_ERR_CUDA;
+  if (tild_check(c, cudaEventRecord(sl.done, c->snap_stream), "snapshot event")) return TILD_ERR_CUDA;
+  sl.ticket.store(t);
+  c->snap_next = t + 1;
+  if (ticket) *ticket = t;
+  return TILD_OK;
+}
+
+// Safe from a writer thread: it reads only the slot's ticket (atomic) and its completion event.
+int snapshot_wait(tild_ctx* c, int64_t ticket) {
+  if (!c || ticket < 0) return TILD_ERR_BAD_INPUT;
+  auto& sl = c->snaps[ticket % TILD_SNAPSHOT_SLOTS];
+  const long long held = sl.ticket.load();
+  if (held < 0 || ticket > held) return TILD_ERR_BAD_INPUT;  // never issued
+  if (ticket < held) return TILD_OK;  // the slot was reused, which waited for this copy first
+  cudaSetDevice(c->device);
+  const cudaError_t e = cudaEventSynchronize(sl.done);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return TILD_ERR_CUDA;
+  }
+  return TILD_OK;
+}
+
 }  // namespace
 
 struct tild_batch : public tild_ctx {};
@@ -1304,6 +1387,27 @@ int32_t tild_batch_create_slots(const tild_config* cfgs, const int32_t* capacity
 }
 int32_t tild_batch_load(tild_batch* b, int32_t sys, const tild_config* cfg) { return sys_load(b, sys, cfg); }
 int32_t tild_autotune(tild_ctx* c, int32_t trial_steps, tild_tune* best) { return engine_autotune(c, trial_steps, best); }
+int32_t tild_snapshot_async(tild_ctx* c, float* x, float* rho, int64_t* ticket) {
+  if (!c) return TILD_ERR_BAD_INPUT;
+  return sys_snapshot_async(c, 0, x, rho, ticket);
+}
+int32_t tild_snapshot_wait(tild_ctx* c, int64_t ticket) { return snapshot_wait(c, ticket); }
+int32_t tild_batch_snapshot_async(tild_batch* b, int32_t sys, float* x, float* rho, int64_t* ticket) {
+  if (!b) return TILD_ERR_BAD_INPUT;
+  return sys_snapshot_async(b, sys, x, rho, ticket);
+}
+int32_t tild_batch_snapshot_wait(tild_batch* b, int64_t ticket) { return snapshot_wait(b, ticket); }
+void* tild_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void tild_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
 int32_t tild_get_tune(tild_ctx* c, tild_tune* out) {
   if (!c || !out) return TILD_ERR_BAD_INPUT;
   get_tune(c, out);

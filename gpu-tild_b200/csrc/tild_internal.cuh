@@ -27,6 +27,7 @@
 #include <stdint.h>
 #include <string>
 #include <vector>
+#include <atomic>
 #include "../../include/tild.h"
 
 #define TILD_MAXT_FAST 4   // k-space kernels are specialised for up to this many channels
@@ -228,6 +229,19 @@ struct tild_ctx {
   double* tab_vr = nullptr;
 
   bool any_stop = false;                 // some system has a device-side stop step
+
+  // asynchronous snapshots (tild_snapshot_async): device buffers captured in stream order, copied
+  // to the host on snap_stream; slot = ticket % TILD_SNAPSHOT_SLOTS
+  struct SnapSlot {
+    float* dx = nullptr;
+    float* drho = nullptr;
+    cudaEvent_t captured = nullptr, done = nullptr;
+    std::atomic<long long> ticket{-1};
+  };
+  cudaStream_t snap_stream = nullptr;
+  SnapSlot snaps[TILD_SNAPSHOT_SLOTS];
+  long long snap_next = 0;
+  size_t snap_x_floats = 0, snap_rho_floats = 0;
 
   long long launches = 0;
   std::string err;

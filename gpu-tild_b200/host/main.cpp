@@ -6,12 +6,18 @@
 // the prefactor ramp applied inside tild_step.  Output files and their text formats follow
 // config_utils.cu:366-403 (traj), io_utils.cu:7-134 (rho%d.dat, avg_sk_%d.dat, binary files),
 // read_input.cu:565-651 (NEED_A_NAME.input) and main.cu:252-265, 422-485 (data.dat, stdout).
-// Steps between two output events are run as one tild_step(n) call.
+// Steps between two output events are run as one tild_step(n) call.  Trajectory, grid and binary
+// frames are snapshotted asynchronously (tild_snapshot_async) and formatted and written by a
+// writer thread while the GPU keeps stepping; files receive the same bytes in the same order.
 //
 // Extra flags (not in the reference): --dry-run parses the script and data file and writes
 // NEED_A_NAME.input without touching a GPU; --device N picks the GPU.
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <ctime>
@@ -33,8 +39,6 @@ struct Run {
   Script s;
   tild_ctx* ctx = nullptr;
   int step = 0;
-  std::vector<float> x;        // host positions [ns*Dim] of the last collect
-  std::vector<float> all_rho;  // host densities [(T+C)*M]
   std::ofstream dout;
   tild_obs obs;
   int M = 1;
@@ -60,18 +64,17 @@ void unstack(const Script& s, int id, int* nn) {  // array_utils.cu:62-81
 }
 
 // write_lammps_traj (config_utils.cu:366-403)
-void write_traj(Run& r) {
-  const Script& s = r.s;
-  FILE* otp = fopen(s.dump_name.c_str(), r.step == 0 ? "w" : "a");
+void write_traj(const Script& s, int step, const float* x) {
+  FILE* otp = fopen(s.dump_name.c_str(), step == 0 ? "w" : "a");
   if (!otp) throw std::runtime_error("cannot open " + s.dump_name);
-  fprintf(otp, "ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\n", r.step, s.sys.ns);
+  fprintf(otp, "ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\n", step, s.sys.ns);
   fprintf(otp, "ITEM: BOX BOUNDS pp pp pp\n");
   fprintf(otp, "%f %f\n%f %f\n%f %f\n", 0.f, s.sys.L[0], 0.f, s.sys.L[1], (s.Dim == 3 ? 0.f : 1.f),
           (s.Dim == 3 ? s.sys.L[2] : 1.f));
   fprintf(otp, s.do_charges ? "ITEM: ATOMS id type mol x y z q\n" : "ITEM: ATOMS id type mol x y z\n");
   for (int i = 0; i < s.sys.ns; i++) {
     fprintf(otp, "%d %d %d  ", i + 1, s.sys.tp[i] + 1, s.sys.molecID[i] + 1);
-    for (int j = 0; j < s.Dim; j++) fprintf(otp, "%f ", r.x[(size_t)i * s.Dim + j]);
+    for (int j = 0; j < s.Dim; j++) fprintf(otp, "%f ", x[(size_t)i * s.Dim + j]);
     for (int j = s.Dim; j < 3; j++) fprintf(otp, "%f", 0.f);
     if (s.do_charges) fprintf(otp, " %f", s.sys.charges[i]);
     fprintf(otp, "\n");
@@ -80,13 +83,12 @@ void write_traj(Run& r) {
 }
 
 // write_grid_data (io_utils.cu:7-32)
-void write_grid(Run& r, const char* name, const float* dat) {
-  const Script& s = r.s;
+void write_grid(const Script& s, int M, const char* name, const float* dat) {
   FILE* otp = fopen(name, "w");
   if (!otp) throw std::runtime_error(std::string("cannot open ") + name);
   const float dx[3] = {s.sys.L[0] / (float)s.Nx[0], s.sys.L[1] / (float)s.Nx[1],
                        s.Dim == 3 ? s.sys.L[2] / (float)s.Nx[2] : 1.f};
-  for (int i = 0; i < r.M; i++) {
+  for (int i = 0; i < M; i++) {
     int nn[3] = {0, 0, 0};
     unstack(s, i, nn);
     for (int j = 0; j < s.Dim; j++) fprintf(otp, "%f ", dx[j] * float(nn[j]));
@@ -141,28 +143,136 @@ void init_binary(Run& r) {
   fclose(otp);
 }
 
-void write_binary(Run& r) {
-  const Script& s = r.s;
+void write_binary(const Script& s, int M, const float* rho, const float* x) {
   FILE* otp = fopen("grid_densities.bin", "ab");
   if (!otp) throw std::runtime_error("Failed to append to grid_densities.bin");
-  fwrite(r.all_rho.data(), sizeof(float), (size_t)r.M * s.sys.ntypes, otp);
+  fwrite(rho, sizeof(float), (size_t)M * s.sys.ntypes, otp);
   fclose(otp);
   otp = fopen("positions.bin", "ab");
   if (!otp) throw std::runtime_error("Failed to append to positions.bin");
-  fwrite(r.x.data(), sizeof(float), (size_t)s.sys.ns * s.Dim, otp);
+  fwrite(x, sizeof(float), (size_t)s.sys.ns * s.Dim, otp);
   fclose(otp);
 }
 
-void collect_x(Run& r) { check(r, tild_get_state(r.ctx, r.x.data(), nullptr, nullptr), "tild_get_state"); }
-void collect_rho(Run& r) { check(r, tild_get_density(r.ctx, r.all_rho.data()), "tild_get_density"); }
-
-void write_rho_files(Run& r) {
-  for (int i = 0; i < r.s.sys.ntypes; i++) {
+void write_rho_files(const Script& s, int M, const float* rho) {
+  for (int i = 0; i < s.sys.ntypes; i++) {
     char nm[30];
     snprintf(nm, sizeof nm, "rho%d.dat", i);
-    write_grid(r, nm, r.all_rho.data() + (size_t)i * r.M);
+    write_grid(s, M, nm, rho + (size_t)i * M);
   }
 }
+
+// Output frames: the state is snapshotted into one of TILD_SNAPSHOT_SLOTS page-locked buffers in
+// stream order, and a writer thread waits for each copy, then formats and writes the frame's files
+// in submission order while the caller keeps stepping.
+class Writer {
+ public:
+  explicit Writer(Run& r) : r_(r) {
+    const size_t nx = (size_t)r.s.sys.ns * r.s.Dim;
+    const size_t nr = (size_t)r.M * (r.s.sys.ntypes + (r.s.do_charges ? 1 : 0));
+    for (int k = 0; k < TILD_SNAPSHOT_SLOTS; k++) {
+      x_[k] = static_cast<float*>(tild_host_alloc(nx * sizeof(float)));
+      rho_[k] = static_cast<float*>(tild_host_alloc(nr * sizeof(float)));
+      if (!x_[k] || !rho_[k]) {  // page-locked memory unavailable: pageable buffers still work
+        tild_host_free(x_[k]);
+        tild_host_free(rho_[k]);
+        x_[k] = rho_[k] = nullptr;
+        fx_[k].assign(nx, 0.f);
+        fr_[k].assign(nr, 0.f);
+      }
+    }
+    th_ = std::thread([this] { loop(); });
+  }
+  ~Writer() {
+    stop();
+    for (int k = 0; k < TILD_SNAPSHOT_SLOTS; k++) {
+      tild_host_free(x_[k]);
+      tild_host_free(rho_[k]);
+    }
+  }
+  // queues the files of one frame: trajectory (x), rho%d.dat (rho), binary frames (x and rho)
+  void frame(int step, bool traj, bool grid, bool bin) {
+    if (!traj && !grid && !bin) return;
+    const int k = (int)(issued_ % TILD_SNAPSHOT_SLOTS);
+    {
+      std::unique_lock<std::mutex> lk(m_);
+      cv_.wait(lk, [&] { return done_ + TILD_SNAPSHOT_SLOTS > issued_ || !err_.empty(); });
+      if (!err_.empty()) throw std::runtime_error(err_);
+    }
+    float* xb = x_[k] ? x_[k] : fx_[k].data();
+    float* rb = rho_[k] ? rho_[k] : fr_[k].data();
+    const bool want_x = traj || bin, want_rho = grid || bin;
+    int64_t ticket = -1;
+    check(r_, tild_snapshot_async(r_.ctx, want_x ? xb : nullptr, want_rho ? rb : nullptr, &ticket),
+          "tild_snapshot_async");
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      q_.push_back({step, traj, grid, bin, ticket, xb, rb});
+      issued_++;
+    }
+    cv_.notify_all();
+  }
+  // waits until every queued frame is on disk
+  void finish() {
+    std::unique_lock<std::mutex> lk(m_);
+    cv_.wait(lk, [&] { return done_ == issued_ || !err_.empty(); });
+    if (!err_.empty()) throw std::runtime_error(err_);
+  }
+
+ private:
+  struct Task {
+    int step;
+    bool traj, grid, bin;
+    int64_t ticket;
+    const float *x, *rho;
+  };
+  void loop() {
+    for (;;) {
+      Task t;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return !q_.empty() || quit_; });
+        if (q_.empty()) return;
+        t = q_.front();
+        q_.pop_front();
+      }
+      try {
+        if (tild_snapshot_wait(r_.ctx, t.ticket) != TILD_OK) throw std::runtime_error("tild_snapshot_wait failed");
+        if (t.traj) write_traj(r_.s, t.step, t.x);
+        if (t.grid) write_rho_files(r_.s, r_.M, t.rho);
+        if (t.bin) write_binary(r_.s, r_.M, t.rho, t.x);
+      } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lk(m_);
+        err_ = e.what();
+      }
+      {
+        std::lock_guard<std::mutex> lk(m_);
+        done_++;
+      }
+      cv_.notify_all();
+    }
+  }
+  void stop() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      quit_ = true;
+    }
+    cv_.notify_all();
+    if (th_.joinable()) th_.join();
+  }
+
+  Run& r_;
+  float* x_[TILD_SNAPSHOT_SLOTS] = {nullptr};
+  float* rho_[TILD_SNAPSHOT_SLOTS] = {nullptr};
+  std::vector<float> fx_[TILD_SNAPSHOT_SLOTS], fr_[TILD_SNAPSHOT_SLOTS];
+  std::thread th_;
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::deque<Task> q_;
+  long long issued_ = 0, done_ = 0;
+  bool quit_ = false;
+  std::string err_;
+};
 
 // print_timestep (main.cu:422-485); values are FP64 here, printed as the reference's floats
 int print_timestep(Run& r) {
@@ -263,14 +373,12 @@ int main(int argc, char** argv) {
                                s.sys.n_bonds.data(), s.sys.bonded_to.data(), s.sys.bond_type.data()),
           "tild_set_topology");
     check(r, tild_set_state(r.ctx, s.sys.x.data(), nullptr, nullptr), "tild_set_state");
-    r.x.assign((size_t)s.sys.ns * s.Dim, 0.f);
-    r.all_rho.assign((size_t)r.M * (s.sys.ntypes + (s.do_charges ? 1 : 0)), 0.f);
     if (s.bin_freq != 0) init_binary(r);
+    Writer writer(r);
     const auto t_init = std::chrono::steady_clock::now();
 
     r.step = 0;
-    collect_x(r);
-    write_traj(r);
+    writer.frame(0, true, false, false);
     r.dout.open("data.dat");
     r.dout << "# step Upe Ubond ";
     if (s.Dim == 2) r.dout << "Pxx Pyy Pxy ";
@@ -282,10 +390,7 @@ int main(int argc, char** argv) {
 
     check(r, tild_forces(r.ctx, nullptr), "tild_forces");
     observables(r);
-    if (s.grid_freq > 0) {
-      collect_rho(r);
-      write_rho_files(r);
-    }
+    writer.frame(0, false, s.grid_freq > 0, false);
     int die_flag = print_timestep(r);
     double io_s = 0.0;
 
@@ -311,19 +416,8 @@ int main(int argc, char** argv) {
         if (r.step > c.wait && c.freq > 0 && r.step % c.freq == 0)
           check(r, tild_sk_accumulate(r.ctx, (int)i, c.type), "tild_sk_accumulate");
       }
-      if (s.traj_freq > 0 && r.step % s.traj_freq == 0) {
-        collect_x(r);
-        write_traj(r);
-      }
-      if (s.grid_freq > 0 && r.step % s.grid_freq == 0) {
-        collect_rho(r);
-        write_rho_files(r);
-      }
-      if (s.bin_freq > 0 && r.step % s.bin_freq == 0) {
-        collect_rho(r);
-        collect_x(r);
-        write_binary(r);
-      }
+      writer.frame(r.step, s.traj_freq > 0 && r.step % s.traj_freq == 0, s.grid_freq > 0 && r.step % s.grid_freq == 0,
+                   s.bin_freq > 0 && r.step % s.bin_freq == 0);
       if (s.log_freq > 0 && r.step % s.log_freq == 0) {
         observables(r);
         die_flag = print_timestep(r);
@@ -341,8 +435,8 @@ int main(int argc, char** argv) {
     }
     // the reference's loop variable ends at max_steps + 1 unless a NaN energy broke the loop
     if (!die_flag) r.step = s.max_steps + 1;
-    collect_x(r);
-    write_traj(r);
+    writer.frame(r.step, true, false, false);
+    writer.finish();
     const auto t_end = std::chrono::steady_clock::now();
     const int dt = (int)std::chrono::duration<double>(t_end - t_main).count();
     std::cout << "Total run time: " << dt / 60 << "m" << dt % 60 << "sec" << std::endl;

@@ -129,6 +129,9 @@ def lib() -> C.CDLL:
         "tild_batch_create_slots": ([C.POINTER(Config), ip, i32, i32, C.POINTER(vp)], i32),
         "tild_batch_capacity": ([vp, i32, ip], i32), "tild_batch_load": ([vp, i32, C.POINTER(Config)], i32),
         "tild_batch_set_stop": ([vp, i32, C.c_int64], i32), "tild_batch_get_active": ([vp, i32, ip], i32),
+        "tild_snapshot_async": ([vp, fp, fp, i64p], i32), "tild_snapshot_wait": ([vp, C.c_int64], i32),
+        "tild_batch_snapshot_async": ([vp, i32, fp, fp, i64p], i32), "tild_batch_snapshot_wait": ([vp, C.c_int64], i32),
+        "tild_host_alloc": ([C.c_size_t], vp), "tild_host_free": ([vp], None),
         "tild_autotune": ([vp, i32, C.POINTER(Tune)], i32), "tild_get_tune": ([vp, C.POINTER(Tune)], i32),
         "tild_set_tune": ([vp, C.POINTER(Tune)], i32), "tild_batch_autotune": ([vp, i32, C.POINTER(Tune)], i32),
         "tild_batch_get_tune": ([vp, C.POINTER(Tune)], i32), "tild_batch_set_tune": ([vp, C.POINTER(Tune)], i32),
@@ -139,6 +142,22 @@ def lib() -> C.CDLL:
         f.restype = res
     _lib = L
     return L
+
+
+class HostArray:
+    """A page-locked float32 host array (tild_host_alloc), freed with the object."""
+
+    def __init__(self, shape):
+        n = int(np.prod(shape))
+        self._p = lib().tild_host_alloc(max(n, 1) * 4)
+        if not self._p:
+            raise MemoryError("page-locked host memory unavailable")
+        self.array = np.ctypeslib.as_array(C.cast(self._p, C.POINTER(C.c_float)), shape=(n,)).reshape(shape)
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().tild_host_free(self._p)
+            self._p = None
 
 
 class TildError(RuntimeError):
@@ -375,6 +394,21 @@ class Context:
         t = Tune()
         self._check(lib().tild_get_tune(self._h, C.byref(t)), "tild_get_tune")
         return t
+
+    def snapshot_async(self, x: Optional[np.ndarray], rho: Optional[np.ndarray]) -> int:
+        """Starts copying the current positions [ns][dim] and/or densities [(T+C)][M] into the given
+        float32 arrays (page-locked ones from host_array overlap with stepping); returns a ticket.
+        The arrays must stay alive and untouched until snapshot_wait(ticket) returns."""
+        for a in (x, rho):
+            if a is not None and (a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("snapshot arrays must be C-contiguous float32")
+        t = C.c_int64()
+        self._check(lib().tild_snapshot_async(self._h, _ptr(x, C.c_float), _ptr(rho, C.c_float), C.byref(t)),
+                    "tild_snapshot_async")
+        return t.value
+
+    def snapshot_wait(self, ticket: int):
+        self._check(lib().tild_snapshot_wait(self._h, int(ticket)), "tild_snapshot_wait")
 
     def set_tune(self, t: Tune):
         self._check(lib().tild_set_tune(self._h, C.byref(t)), "tild_set_tune")

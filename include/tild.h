@@ -27,6 +27,7 @@
 #ifndef TILD_H
 #define TILD_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -301,6 +302,26 @@ int32_t tild_autotune(tild_ctx* ctx, int32_t trial_steps, tild_tune* best);
 int32_t tild_batch_autotune(tild_batch* b, int32_t trial_steps, tild_tune* best);
 int32_t tild_batch_get_tune(tild_batch* b, tild_tune* out);
 int32_t tild_batch_set_tune(tild_batch* b, const tild_tune* t);
+
+/* ---- asynchronous snapshots for output writers ----------------------------------------------- */
+/* The reference copies positions and densities to the host and formats its output files between
+ * steps with the device idle (cuda_collect_x / cuda_collect_rho, device_comm_utils.cu:20-37;
+ * write_lammps_traj, config_utils.cu:366-403; write_binary, io_utils.cu:85-134).  Here a snapshot
+ * captures the current positions x[ns][Dim] (bead order) and/or the densities rho[(T+C)][M] of the
+ * last force evaluation into a device buffer in stream order, and a separate copy stream moves
+ * them to the host arrays while the context keeps stepping.  x or rho may be NULL.  Host arrays
+ * should be page-locked (tild_host_alloc) for the copy to overlap with stepping.  *ticket names
+ * the snapshot; tild_snapshot_wait(ctx, ticket) blocks until it is in the host arrays and may be
+ * called from a writer thread other than the one driving the context.  At most
+ * TILD_SNAPSHOT_SLOTS snapshots are in flight: a further call first waits for the oldest. */
+#define TILD_SNAPSHOT_SLOTS 4
+int32_t tild_snapshot_async(tild_ctx* ctx, float* x, float* rho, int64_t* ticket);
+int32_t tild_snapshot_wait(tild_ctx* ctx, int64_t ticket);
+int32_t tild_batch_snapshot_async(tild_batch* b, int32_t sys, float* x, float* rho, int64_t* ticket);
+int32_t tild_batch_snapshot_wait(tild_batch* b, int64_t ticket);
+/* Page-locked host memory (cudaMallocHost / cudaFreeHost); NULL when it cannot be had. */
+void* tild_host_alloc(size_t bytes);
+void tild_host_free(void* p);
 
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device memory (code that
