@@ -65,6 +65,22 @@ class JobResult:
         return self.finished - self.arrival
 
 
+@dataclasses.dataclass
+class Checkpoint:
+    """Full state of a preempted job: resuming it in any free slot of its grid shape continues
+    the trajectory bitwise (positions, x_{n-1} and GJF noise restored, step counter restored, the
+    noise being keyed by (bead id, step, seed)).  avg_sk is carried as the accumulated sum."""
+    job: Job
+    result: JobResult
+    x: np.ndarray
+    xo: np.ndarray
+    noise: np.ndarray
+    step: int
+    sk_sum: Optional[np.ndarray]
+    sk_calls: int
+    epochs_run: int = 0
+
+
 def grid_edge(s: tild.System) -> int:
     nx = tuple(int(v) for v in s.nx[:s.dim])
     if len(set(nx)) != 1:
@@ -134,43 +150,77 @@ class Server:
         self.close()
 
     # ---------------------------------------------------------------------------------------
-    def run(self, jobs: Sequence[Job], clock: str = "wall") -> List[JobResult]:
+    def checkpoint(self, slot: int, job: Job, r: JobResult, epochs_run: int = 0) -> Checkpoint:
+        """Takes the full state of the job in `slot` off the GPU and frees the slot."""
+        x, xo, nz = self.batch.get_state(slot)
+        sk, n = self.batch.sk_get(slot, 0)
+        ck = Checkpoint(job, r, x, xo, nz, self.batch.step_count(slot), sk * n if n else None, n, epochs_run)
+        self.batch.set_active(slot, False)
+        self.free[r.grid].append(slot)
+        return ck
+
+    def _start(self, slot: int, item, now: float):
+        """Puts a new job or a checkpoint into `slot` and activates it."""
+        if isinstance(item, Checkpoint):
+            job, r = item.job, item.result
+            self.batch.load(slot, job.system, activate=False)
+            self.batch.set_state(slot, item.x, item.xo, item.noise)
+            self.batch.set_step(slot, item.step)
+            r.slot = slot
+        else:
+            job = item
+            r = JobResult(job.job_id, job.system.ns, grid_edge(job.system), job.steps, job.arrival, admitted=now,
+                          slot=slot)
+            self.batch.load(slot, job.system, activate=False)
+        self.batch.set_stop(slot, job.steps)
+        self.batch.set_active(slot, True)
+        return job, r
+
+    def run(self, jobs: Sequence[Job], clock: str = "wall", time_slice: Optional[int] = None,
+            preempt_at: Optional[Dict[int, int]] = None) -> List[JobResult]:
         """Serves `jobs` to completion.  clock="wall": arrivals in seconds of wall time since the
         call (a Poisson stream replayed in real time); clock="epochs": arrival k means the job
         arrives before epoch k (deterministic, for tests).  Times in the results use the same
-        unit as the arrivals."""
+        unit as the arrivals.
+
+        time_slice: a job that has run this many epochs while another job of its grid shape
+        waits is checkpointed and queued behind it (round-robin within a shape); None never
+        preempts.  preempt_at: {job_id: epoch} checkpoints that job once, after that many of its
+        epochs (tests)."""
         for j in jobs:
             if grid_edge(j.system) not in self.free:
                 raise ValueError(f"job {j.job_id}: no slot has grid edge {grid_edge(j.system)}")
             if j.steps < 1:
                 raise ValueError(f"job {j.job_id}: steps must be positive")
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
-        queue: List[Job] = []
-        running: Dict[int, tuple] = {}
+        queue: List = []                      # Jobs and Checkpoints, first come first served
+        running: Dict[int, list] = {}         # slot -> [job, result, epochs run since (re)start]
         results: Dict[int, JobResult] = {}
+        sk_parts: Dict[int, list] = collections.defaultdict(list)
+        preempt_at = dict(preempt_at or {})
         t0 = time.perf_counter()
         epoch_no = 0
 
         def now() -> float:
             return (time.perf_counter() - t0) if clock == "wall" else float(epoch_no)
 
+        def edge_of(item) -> int:
+            return grid_edge((item.job if isinstance(item, Checkpoint) else item).system)
+
         while pending or queue or running:
             t = now()
             while pending and pending[0].arrival <= t:
                 queue.append(pending.popleft())
             waiting = []
-            for job in queue:
-                g = grid_edge(job.system)
+            for item in queue:
+                g = edge_of(item)
                 if self.free[g]:
                     slot = self.free[g].popleft()
-                    self.batch.load(slot, job.system, activate=False)
-                    self.batch.set_stop(slot, job.steps)
-                    self.batch.set_active(slot, True)
-                    r = JobResult(job.job_id, job.system.ns, g, job.steps, job.arrival, admitted=now(), slot=slot)
-                    running[slot] = (job, r)
+                    job, r = self._start(slot, item, now())
+                    running[slot] = [job, r, 0]
                     results[job.job_id] = r
                 else:
-                    waiting.append(job)
+                    waiting.append(item)
             queue = waiting
             if not running:
                 if pending and clock == "wall":
@@ -185,18 +235,36 @@ class Server:
             self.stepping_s += time.perf_counter() - ts0
             self.epochs_run += 1
             epoch_no += 1
+            waiting_edges = collections.Counter(edge_of(it) for it in queue)
             for slot in list(running):
-                job, r = running[slot]
+                job, r, ran = running[slot]
+                ran += 1
+                running[slot][2] = ran
                 o = self.batch.observables(slot)
                 r.energy.append((self.batch.step_count(slot), o["upe"]))
                 self.batch.sk_accumulate(slot, 0, job.sk_type)
                 if not self.batch.active(slot):
-                    r.sk, r.sk_calls = self.batch.sk_get(slot, 0)
+                    sk, n = self.batch.sk_get(slot, 0)
+                    parts = sk_parts.pop(job.job_id, []) + [(sk * n, n)]
+                    r.sk_calls = sum(k for _, k in parts)
+                    r.sk = sum(v for v, _ in parts) / r.sk_calls
                     if self.keep_positions:
                         r.x = self.batch.get_state(slot)[0]
                     r.finished = now()
                     del running[slot]
                     self.free[r.grid].append(slot)
+                    continue
+                forced = preempt_at.get(job.job_id) == ran
+                if forced or (time_slice is not None and ran >= time_slice and waiting_edges[r.grid] > 0):
+                    if forced:
+                        del preempt_at[job.job_id]
+                    ck = self.checkpoint(slot, job, r)
+                    if ck.sk_sum is not None:
+                        sk_parts[job.job_id].append((ck.sk_sum, ck.sk_calls))
+                    ck.sk_sum, ck.sk_calls = None, 0
+                    del running[slot]
+                    queue.append(ck)
+                    waiting_edges[r.grid] -= 1
         return [results[j.job_id] for j in jobs]
 
 

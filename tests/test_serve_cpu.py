@@ -65,7 +65,17 @@ class FakeBatch:
         return self.act[i]
 
     def sk_get(self, i, slot):
-        return np.zeros(4, np.complex128), self.sk[i]
+        return np.ones(4, np.complex128), self.sk[i]
+
+    def get_state(self, i):
+        x = np.full((self.systems[i].ns, 3), float(self.stepc[i]), np.float32)
+        return x, x.copy(), x.copy()
+
+    def set_state(self, i, x, xo=None, noise=None):
+        pass
+
+    def set_step(self, i, n):
+        self.stepc[i] = n
 
 
 class FakeServer(sv.Server):
@@ -120,3 +130,16 @@ def test_poisson_stream_and_capacity():
         g = sv.grid_edge(j.system)
         assert g in ts.ensemble_grid_edges()
         assert j.system.ns <= ts.ensemble_capacity(g)
+
+
+def test_time_slice_preempts_and_resumes_from_checkpoints():
+    srv = FakeServer({24: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                     measure_memory=False)
+    jobs = [sv.Job(0, tiny(24, 2), 256, 0), sv.Job(1, tiny(24, 3), 128, 0)]
+    res = srv.run(jobs, clock="epochs", time_slice=1)
+    by = {r.job_id: r for r in res}
+    # one slot, slices of one epoch: the two jobs alternate until job 1 (2 epochs) is done
+    assert [s for s, _ in by[0].energy] == [64, 128, 192, 256]
+    assert [s for s, _ in by[1].energy] == [64, 128]
+    assert by[1].finished == 4 and by[0].finished == 6
+    assert by[0].sk_calls == 4 and by[1].sk_calls == 2

@@ -94,3 +94,20 @@ def test_served_results_same_alone_and_in_mix():
         assert np.allclose(rm.sk, ra.sk, rtol=1e-4, atol=1e-6 * np.abs(ra.sk).max())
     print(f"alone vs mix: max energy rel diff {worst_e:.3e}, max position diff {worst_x:.3e}")
     assert worst_e < ENERGY_RTOL and worst_x < POS_ATOL
+
+
+def test_preempted_job_resumes_bitwise():
+    """A job checkpointed off the GPU mid-run and resumed later in a slot that another job used in
+    between gives the same energy trace and final positions as the same job run without a break."""
+    a = sv.Job(0, job_system(24, 31), 320, 0)
+    b = sv.Job(1, job_system(24, 32, N=10), 128, 0)
+    with sv.Server({24: 1}, epoch=64, keep_positions=True, measure_memory=False) as srv:
+        broken = srv.run([a, b], clock="epochs", preempt_at={0: 2})
+    with sv.Server({24: 1}, epoch=64, keep_positions=True, measure_memory=False) as srv:
+        whole = srv.run([sv.Job(0, a.system, a.steps, 0)], clock="epochs")[0]
+    ra = broken[0]
+    assert ra.admitted == 0 and ra.finished > whole.finished       # it waited while job 1 ran
+    assert ra.energy == whole.energy
+    assert np.array_equal(ra.x, whole.x)
+    assert ra.sk_calls == whole.sk_calls
+    assert np.allclose(ra.sk, whole.sk, rtol=1e-12, atol=1e-12 * np.abs(whole.sk).max())
