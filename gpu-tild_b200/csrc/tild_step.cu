@@ -557,7 +557,7 @@ __device__ __forceinline__ void bead_epilogue(int i, const float4& p, int t, flo
 }
 
 template <int D, int P, bool INTEG, bool XW>
-__global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 2 ? 3 : 4))) k_gather(
+__global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 : 4)))) k_gather(
     const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
