@@ -399,6 +399,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   }
   // channel layout: bucket by bucket so each bucket is one batched transform
   long long grid = 0, spec = 0;
+  long long g4tot = 0;
   for (Bucket& b : c->buckets) {
     b.grid0 = grid;
     b.spec0 = spec;
@@ -407,8 +408,13 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
       SysHost& h = c->sys[s];
       h.grid0 = grid;
       h.spec0 = spec;
+      h.Mb = tild_field_stride(h.g, h.D);
+      h.g4_0 = g4tot;
+      g4tot += (long long)(h.T + h.C) * h.Mb;
       c->h_sys[s].grid0 = grid;
       c->h_sys[s].spec0 = spec;
+      c->h_sys[s].g4_0 = h.g4_0;
+      c->h_sys[s].Mb = h.Mb;
       grid += (long long)(h.T + h.C) * h.g.M;
       spec += (long long)(h.T + h.C) * h.g.Mh;
       b.channels += h.T + h.C;
@@ -416,6 +422,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   }
   c->grid_total = grid;
   c->spec_total = spec;
+  c->g4_total = g4tot;
   c->nslots = (int)slots;
   c->nbeads = (int)beads;
   // CTA -> system lookup tables (grid and spectrum tables carry each system's first block after them)
@@ -451,7 +458,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   rc = rc ? rc : dalloc(c, &c->rhok, (size_t)spec, "density spectra");
   rc = rc ? rc : dalloc(c, &c->gk, (size_t)spec * c->D, "force spectra");
   rc = rc ? rc : dalloc(c, &c->gfield, (size_t)grid * c->D, "force fields");
-  rc = rc ? rc : dalloc(c, &c->g4, (size_t)grid, "interleaved force fields");
+  rc = rc ? rc : dalloc(c, &c->g4, (size_t)c->g4_total, "interleaved force fields");
   rc = rc ? rc : dalloc(c, &c->utab, (size_t)utab, "multiplier tables");
   rc = rc ? rc : dalloc(c, &c->virk, (size_t)virk, "virial tables");
   if (ctab) rc = rc ? rc : dalloc(c, &c->ctab, (size_t)ctab, "charge table");
@@ -920,6 +927,7 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
   t->gather_mode = c->gather_mode;
   t->gather_cap = c->gather_cap;
   t->sort_brick = c->sort_brick;
+  t->field_layout = c->field_layout;
   t->ms_per_step = 0.0;
 }
 
@@ -927,7 +935,8 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
   if (!t || (t->spread_mode != TILD_SPREAD_TILED && t->spread_mode != TILD_SPREAD_DIRECT) || t->spread_cap < 1024 ||
       t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
       t->gather_mode < TILD_GATHER_DIRECT || t->gather_mode > TILD_GATHER_BOX || t->gather_cap < 1024 ||
-      t->gather_cap > 3072)
+      t->gather_cap > 3072 || t->field_layout < TILD_FIELD_LINEAR || t->field_layout > TILD_FIELD_BRICK ||
+      (t->field_layout == TILD_FIELD_BRICK && c->D != 3))
     return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
   if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
   {
@@ -941,6 +950,7 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
   c->spread_cap = t->spread_cap;
   c->gather_mode = t->gather_mode;
   c->gather_cap = t->gather_cap;
+  c->field_layout = t->field_layout;
   if (t->sort_brick != c->sort_brick) {
     c->sort_brick = t->sort_brick;
     c->steps_since_sort = c->sort_interval;  // re-sort with the new keys at the next step
@@ -1014,6 +1024,12 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
         tild_tune t = cur;
         t.spread_cap = cap;
         if (cap != cur.spread_cap) consider(t);
+      }
+    if (c->D == 3)
+      for (int layout : {TILD_FIELD_LINEAR, TILD_FIELD_BRICK}) {
+        tild_tune t = cur;
+        t.field_layout = layout;
+        if (layout != cur.field_layout) consider(t);
       }
     for (int mode : {TILD_GATHER_DIRECT, TILD_GATHER_BOX}) {
       tild_tune t = cur;

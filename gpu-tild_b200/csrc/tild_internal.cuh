@@ -60,6 +60,7 @@ struct SysDev {
   int active;                      // 0: skipped by the particle kernels
   long long grid0;                 // channel 0 of this system in rho / rho_fx / g4 (grid points)
   long long spec0;                 // channel 0 in rhok (half-spectrum points)
+  long long g4_0, Mb;              // channel 0 in g4 and the per-channel stride there (>= M)
   long long utab0, ctab0, kd0;     // offsets in utab, ctab, kd
   long long step;                  // completed steps (advanced on the device)
   long long stop_at;               // the system turns inactive once step reaches it (-1: never)
@@ -90,6 +91,7 @@ struct SysHost {
   int slot0 = 0, ns_pad = 0, bead0 = 0;  // bead0: first bead in the engine's bead numbering
   int cap = 0;                           // beads the slot can hold (>= ns; tild_batch_load)
   long long grid0 = 0, spec0 = 0, utab0 = 0, ctab0 = 0, kd0 = 0, virk0 = 0;
+  long long g4_0 = 0, Mb = 0;            // force-field storage (tild_field_stride)
   int kbits = 20;
   std::vector<int> fft_cfg;              // fft table slot -> config style index
   int type_integ_mask[TILD_MAX_TYPES] = {0};
@@ -124,6 +126,8 @@ struct tild_ctx {
   int gather_mode = TILD_GATHER_DIRECT;  // order >= 2: stencil reads from global memory or shared boxes
   int gather_cap = 2048;                 // float4 nodes of a gather box buffer, 1024..3072
   int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
+  int field_layout = TILD_FIELD_LINEAR;  // node order of the float4 force field g4
+  long long g4_total = 0;
   int D = 3, P = 1;
   int nsys = 1;
   std::vector<SysHost> sys;
@@ -264,6 +268,23 @@ inline void tild_mark(tild_ctx* c, int stage) {
 }
 
 // ---- small helpers -----------------------------------------------------------------------
+// Per-channel storage of the float4 force field: room for the brick layout (3D: 4x4x4 bricks,
+// edges rounded up to 4), so either layout fits without reallocating.
+inline long long tild_field_stride(const Geom& g, int D) {
+  if (D != 3) return g.M;
+  return (long long)((g.nx[0] + 3) / 4) * ((g.nx[1] + 3) / 4) * ((g.nx[2] + 3) / 4) * 64;
+}
+
+// Offset of node n along axis d in one channel of the force field.  Linear: x fastest.  Brick
+// (3D): 4x4x4 bricks of 64 consecutive nodes (1 KB), bricks x fastest, so the stencil loads of a
+// warp of spatially sorted beads fall in a few contiguous blocks.
+__device__ __forceinline__ int tild_field_off(int layout, int d, int n, const Geom& g) {
+  if (layout == TILD_FIELD_LINEAR) return d == 0 ? n : (d == 1 ? n * g.nx[0] : n * g.nx[0] * g.nx[1]);
+  const int nbx = (g.nx[0] + 3) >> 2, nby = (g.nx[1] + 3) >> 2;
+  if (d == 0) return ((n >> 2) << 6) | (n & 3);
+  if (d == 1) return (((n >> 2) * nbx) << 6) | ((n & 3) << 2);
+  return (((n >> 2) * nbx * nby) << 6) | ((n & 3) << 4);
+}
 __device__ __forceinline__ int tild_type_of(float w) { return __float_as_int(w) & 0xff; }
 
 // spline_get_weights (device_grid_utils.cu:3-49), FP32, including the order-4 quirk

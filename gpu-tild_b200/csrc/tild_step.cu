@@ -415,19 +415,27 @@ __global__ void k_fieldphase_apply(float* __restrict__ gfield, const float* __re
 template <int D>
 __global__ void k_interleave(const float* __restrict__ planar_all, float4* __restrict__ g4_all,
                              const int* __restrict__ cta_sys, const int* __restrict__ blk0,
-                             const SysDev* __restrict__ sysd) {
+                             const SysDev* __restrict__ sysd, int layout) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
   if (!sd.active) return;  // inactive systems are not gathered
-  const long long M = sd.g.M;
+  const Geom& g = sd.g;
+  const long long M = g.M;
   const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
   if (m >= M) return;
+  long long dst = m;
+  if (layout != TILD_FIELD_LINEAR) {
+    const int x = (int)(m % g.nx[0]);
+    const long long r = m / g.nx[0];
+    const int y = (int)(r % g.nx[1]), z = (int)(r / g.nx[1]);
+    dst = tild_field_off(layout, 0, x, g) + tild_field_off(layout, 1, y, g) + tild_field_off(layout, 2, z, g);
+  }
   const float* planar = planar_all + sd.grid0 * D;
-  float4* g4 = g4_all + sd.grid0;
+  float4* g4 = g4_all + sd.g4_0;
   const int nch = sd.T + sd.C;
   for (int ch = 0; ch < nch; ch++) {
     const float* src = planar + (long long)ch * D * M + m;
-    g4[(long long)ch * M + m] = make_float4(src[0], src[M], D == 3 ? src[2 * M] : 0.f, 0.f);
+    g4[(long long)ch * sd.Mb + dst] = make_float4(src[0], src[M], D == 3 ? src[2 * M] : 0.f, 0.f);
   }
 }
 
@@ -438,17 +446,17 @@ __global__ void k_interleave(const float* __restrict__ planar_all, float4* __res
 // ---------------------------------------------------------------------------------------------
 template <int D, int P>
 __device__ __forceinline__ void gather4(const float4* __restrict__ F, const float (&W)[3][P + 1],
-                                        const int (&idx)[3][P + 1], const Geom& g, float (&acc)[3]) {
+                                        const int (&o)[3][P + 1], float (&acc)[3]) {
 #pragma unroll
   for (int ix = 0; ix <= P; ix++)
 #pragma unroll
     for (int iy = 0; iy <= P; iy++) {
       const float wxy = W[0][ix] * W[1][iy];
-      const long long row = idx[0][ix] + (long long)idx[1][iy] * g.nx[0];
+      const int row = o[0][ix] + o[1][iy];
       if (D == 3) {
 #pragma unroll
         for (int iz = 0; iz <= P; iz++) {
-          const float4 v = __ldg(F + row + (long long)idx[2][iz] * g.nx[1] * g.nx[0]);
+          const float4 v = __ldg(F + row + o[2][iz]);
           const float w = wxy * W[2][iz];
           acc[0] += v.x * w;
           acc[1] += v.y * w;
@@ -460,6 +468,16 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ F, const floa
         acc[1] += v.y * wxy;
       }
     }
+}
+
+// stencil node indices -> offsets in one channel of the force field
+template <int D, int P>
+__device__ __forceinline__ void field_offsets(const int (&idx)[3][P + 1], int layout, const Geom& g,
+                                              int (&o)[3][P + 1]) {
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int a = 0; a <= P; a++) o[d][a] = d < D ? tild_field_off(layout, d, idx[d][a], g) : 0;
 }
 
 // Bonds, the force output and the integrators of one bead: d_bonds (device_bonds.cu:4-60) and
@@ -562,7 +580,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 :
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
     const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
-    int* status) {
+    int layout, int* status) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -579,9 +597,9 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 :
     return;  // left in place; the host reports TILD_ERR_NAN
   }
   const Geom& g = sd.g;
-  const long long M = g.M;
+  const long long Mb = sd.Mb;
   const int T = sd.T, C = sd.C;
-  const float4* g4 = g4_all + sd.grid0;
+  const float4* g4 = g4_all + sd.g4_0;
   // loads that do not depend on the stencil are issued before it, so their latency overlaps
   const int info = bond_info[i];
   const int nb = info & 3;
@@ -603,16 +621,18 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 :
 #pragma unroll
       for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
     }
+    int o[3][P + 1];
+    field_offsets<D, P>(idx, layout, g, o);
     if (C) {
       const float q = charge[i];
       if (q != 0.f) {
         float e[3] = {0.f, 0.f, 0.f};
-        gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
+        gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
 #pragma unroll
         for (int d = 0; d < D; d++) f[d] += e[d] * q;
       }
     }
-    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
+    gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
   }
   bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
 }
@@ -701,9 +721,9 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
   int mn[3], ext[3];
   long long vol;
   if (!chunk_box<D, P>(ok, rel, s_min, s_max, mn, ext, vol)) return;
-  const long long M = g.M;
+  const long long Mb = sd.Mb;  // the box gather runs on the linear layout
   const int T = sd.T, C = sd.C, nch = T + C;
-  const float4* g4 = g4_all + sd.grid0;
+  const float4* g4 = g4_all + sd.g4_0;
   const float q = (C && ok) ? charge[i] : 0.f;
   float f[3] = {0.f, 0.f, 0.f};
   const int ex = ext[0], ey = ext[1], ez = ext[2];
@@ -733,7 +753,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
     if (my_r < rpi)
       for (int R = warp * rpi + my_r; R < nrows; R += nwarps * rpi) {
         const int ch = R / rows, yz = R - ch * rows;
-        const float4* src = g4 + (long long)ch * M + s_row[yz];
+        const float4* src = g4 + (long long)ch * Mb + s_row[yz];
         float4* dst = sbox + (long long)ch * vol + (long long)yz * ex;
 #pragma unroll
         for (int k = 0; k < 2; k++) {
@@ -760,13 +780,15 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
     for (int d = 0; d < D; d++)
 #pragma unroll
       for (int a = 0; a <= P; a++) idx[d][a] = pmod(base[d] + a, g.nx[d]);
+    int o[3][P + 1];
+    field_offsets<D, P>(idx, TILD_FIELD_LINEAR, g, o);
     if (C && q != 0.f) {
       float e[3] = {0.f, 0.f, 0.f};
-      gather4<D, P>(g4 + (long long)T * M, W, idx, g, e);
+      gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
 #pragma unroll
       for (int d = 0; d < D; d++) f[d] += e[d] * q;
     }
-    gather4<D, P>(g4 + (long long)t * M, W, idx, g, f);
+    gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
   }
   if (!ok) return;
   bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
@@ -805,7 +827,7 @@ void launch_spread(tild_ctx* c) {
 
 template <int D, int P, bool I, bool X>
 void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
-  if (P >= 2 && c->gather_mode == TILD_GATHER_BOX) {
+  if (P >= 2 && c->gather_mode == TILD_GATHER_BOX && c->field_layout == TILD_FIELD_LINEAR) {
     static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
     if (!(attr_devices >> (c->device & 63) & 1ull)) {
       cudaFuncSetAttribute(k_gather_box<D, P, I, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -819,7 +841,7 @@ void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
   }
   k_gather<D, P, I, X><<<c->n_cta_bead, kTile, 0, c->stream>>>(
       c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
-      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->d_status);
+      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->d_status);
 }
 
 template <int D, int P>
@@ -928,8 +950,10 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   tild_mark(c, STAGE_INTERLEAVE);
   {
     int* blk0 = c->cta_grid + c->n_cta_grid;
-    if (c->D == 3) k_interleave<3><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
-    else k_interleave<2><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys);
+    if (c->D == 3)
+      k_interleave<3><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout);
+    else
+      k_interleave<2><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout);
     c->launches++;
   }
   tild_mark(c, STAGE_GATHER);

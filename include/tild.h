@@ -278,6 +278,7 @@ int32_t tild_batch_get_active(tild_batch* b, int32_t sys, int32_t* active);
  * them. */
 enum { TILD_SPREAD_TILED = 0, TILD_SPREAD_DIRECT = 1 };
 enum { TILD_GATHER_DIRECT = 0, TILD_GATHER_BOX = 1 };
+enum { TILD_FIELD_LINEAR = 0, TILD_FIELD_BRICK = 1 };
 typedef struct tild_tune {
   int32_t spread_mode;    /* order >= 2: shared-memory box per 256 beads (TILED) or 64-bit global atomics (DIRECT) */
   int32_t spread_cap;     /* shared box of the tiled spread, 32-bit words, 1024..12288 */
@@ -289,12 +290,14 @@ typedef struct tild_tune {
   int32_t sort_brick;     /* sort key bricks: log2 edges x | y<<4 | z<<8, bit 12 = Morton order of the
                              bricks; 3D 0x222 (default), 0x1222, 0x1113, 0x1123; 2D 0x033 (default),
                              0x1033, 0x1014 */
+  int32_t field_layout;   /* node order of the force field the gather reads: x-fastest (LINEAR) or 4x4x4
+                             bricks of consecutive nodes (BRICK, 3D; the box gather needs LINEAR) */
   double ms_per_step;     /* tild_autotune: measured step time with these settings */
 } tild_tune;
 int32_t tild_get_tune(tild_ctx* ctx, tild_tune* out);
 int32_t tild_set_tune(tild_ctx* ctx, const tild_tune* t);
-/* Times candidate settings (coordinate descent over spread mode and box, gather mode and box, sort
- * bricks, sort interval and FFT streams, each trial trial_steps steps after one graph period of warm-up) and keeps the fastest.
+/* Times candidate settings (coordinate descent over spread mode and box, gather mode and box, force
+ * field layout, sort bricks, sort interval and FFT streams, each trial trial_steps steps after one graph period of warm-up) and keeps the fastest.
  * The state of every system (positions, x_{n-1}, noise, step counters, activity) is restored
  * afterwards, so tuning does not advance the simulation.  Not available with TILD_RNG_XORWOW (the
  * generator states would advance). */

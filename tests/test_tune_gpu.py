@@ -34,6 +34,8 @@ def run(s, tune=None, steps=70):
     {"sort_brick": 0x1123, "sort_interval": 8},
     {"gather_mode": tild.GATHER_BOX},
     {"gather_mode": tild.GATHER_BOX, "gather_cap": 1024},   # most chunks fall back to global reads
+    {"field_layout": tild.FIELD_BRICK},
+    {"field_layout": tild.FIELD_BRICK, "gather_mode": tild.GATHER_BOX},   # box needs linear: direct runs
 ])
 def test_every_setting_gives_the_same_trajectory(tune):
     s = p3_system()
