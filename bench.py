@@ -242,7 +242,7 @@ def step_bytes(s) -> int:
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch of the stage's kernel, from one ncu
 # capture of that kernel on the same workload (summaries and commands under profiles/)
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 290827776, "spread": 75483392},
+    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 298451456, "spread": 75735808},
 }
 
 

@@ -1034,6 +1034,7 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
     for (int mode : {TILD_GATHER_DIRECT, TILD_GATHER_BOX}) {
       tild_tune t = cur;
       t.gather_mode = mode;
+      if (mode == TILD_GATHER_BOX && cur.field_layout != TILD_FIELD_LINEAR) continue;  // box reads the linear field
       if (mode != cur.gather_mode) consider(t);
     }
     if (cur.gather_mode != TILD_GATHER_DIRECT)
