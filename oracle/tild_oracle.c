@@ -457,7 +457,7 @@ static void weights(double gdx, double H, double* W, int p) {
 static int bead_stencil(const orc_sys* s, const float* xb, int* inds, double* w) {
   const int D = s->D, p = s->p;
   int g[3] = {0, 0, 0};
-  double W[3][6];
+  double W[3][6] = {{0}};
   for (int j = 0; j < D; j++) {
     float xj = xb[j], dxj = s->dx[j];
     double gdx;
