@@ -323,8 +323,6 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   }
   c->device = device;
   if (tild_check(c, cudaSetDevice(device), "cudaSetDevice")) return TILD_ERR_CUDA;
-  if (tild_check(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "device attribute"))
-    return TILD_ERR_CUDA;
   if (tild_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream")) return TILD_ERR_CUDA;
   c->D = cfgs[0].dim;
   c->P = cfgs[0].pmeorder;

@@ -114,7 +114,6 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
 
 struct tild_ctx {
   int device = 0;
-  int num_sms = 148;
   cudaStream_t stream = nullptr;
   // auxiliary streams: the FFTs of different grid shapes run concurrently (fork/join by events)
   std::vector<cudaStream_t> aux;

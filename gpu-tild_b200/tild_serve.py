@@ -135,7 +135,8 @@ class Server:
             self.free[g].append(i)
         self.nslots = len(systems)
         self.epochs_run = 0
-        self.stepping_s = 0.0
+        self.stepping_s = 0.0     # wall time of the stepping calls and their force evaluation
+        self.work_done = 0        # particle-steps the jobs advanced inside those calls
 
     def _make_batch(self, systems, caps):
         return tild.Batch(systems, device=self.device, capacity=caps)
@@ -229,6 +230,7 @@ class Server:
                     epoch_no = max(epoch_no + 1, int(math.ceil(pending[0].arrival)))
                 continue
             ts0 = time.perf_counter()
+            before = {slot: self.batch.step_count(slot) for slot in running}
             self.batch.step(self.epoch)
             # records describe each job's state after the epoch (stopped jobs: their last step)
             self.batch.evaluate()
@@ -241,7 +243,9 @@ class Server:
                 ran += 1
                 running[slot][2] = ran
                 o = self.batch.observables(slot)
-                r.energy.append((self.batch.step_count(slot), o["upe"]))
+                step_now = self.batch.step_count(slot)
+                self.work_done += (step_now - before[slot]) * job.system.ns
+                r.energy.append((step_now, o["upe"]))
                 self.batch.sk_accumulate(slot, 0, job.sk_type)
                 if not self.batch.active(slot):
                     sk, n = self.batch.sk_get(slot, 0)
