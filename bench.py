@@ -72,7 +72,7 @@ def run_ensemble(args):
     local = [systems[i] for i in mine]
     B = tild.Batch(local, device=grp.local)
     schedule = None if args.no_tune else B.autotune(trial_steps=64)
-    period = graph_period(B.get_tune())
+    period = int(grp.max(graph_period(B.get_tune())))  # the same step count on every rank
     args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
     B.step(-(-args.warmup * 32 // period) * period)
     B.sync()
@@ -316,7 +316,7 @@ def run_ours(args):
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
     schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
-    period = graph_period(ctx.get_tune())
+    period = int(grp.max(graph_period(ctx.get_tune())))  # the same step count on every rank
     args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
     ctx.step(args.warmup)
     ctx.sync()
