@@ -665,9 +665,10 @@ int run_steps(tild_ctx* c, int n) {
       c->steps_since_sort = c->sort_interval;  // the graph always starts with a sort
       const void* p0 = c->pos[0];
       const int cur = c->cur;
+      const std::vector<char> on = tild_buckets_on(c);
       cudaGraphExec_t exec = nullptr;
       for (auto& ge : c->graphs)
-        if (ge.p0 == p0 && ge.cur == cur) exec = ge.exec;
+        if (ge.p0 == p0 && ge.cur == cur && ge.buckets_on == on) exec = ge.exec;
       if (!exec) {
         const long long l0 = c->launches;
         const int64_t step_before = c->sys[0].step;
@@ -700,7 +701,11 @@ int run_steps(tild_ctx* c, int n) {
         c->h_sys = saved_hsys;
         c->sorts = saved_sorts;
         c->launches = l0;
-        c->graphs.push_back({exec, p0, cur});
+        if (c->graphs.size() >= 8) {  // keep the eight most recent configurations
+          cudaGraphExecDestroy(c->graphs.front().exec);
+          c->graphs.erase(c->graphs.begin());
+        }
+        c->graphs.push_back({exec, p0, cur, on});
         c->graph_launches_per_step = per_step;
         // after capture the buffer configuration is back at (p0, cur): same as a replay
       }

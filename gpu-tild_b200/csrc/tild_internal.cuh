@@ -207,6 +207,7 @@ struct tild_ctx {
     cudaGraphExec_t exec;
     const void* p0;
     int cur;
+    std::vector<char> buckets_on;        // grid shapes whose transforms the graph runs
   };
   std::vector<GraphEntry> graphs;
   bool use_graphs = true;
@@ -397,6 +398,19 @@ int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);
 int tild_assign_lanes(tild_ctx* c, int lanes);
+
+// Grid shapes with at least one active system: integrating steps skip the transforms of the others
+// (their systems neither move nor are gathered).  Force-only evaluations transform every shape.
+inline std::vector<char> tild_buckets_on(const tild_ctx* c) {
+  std::vector<char> on(c->buckets.size(), 0);
+  for (size_t b = 0; b < c->buckets.size(); b++)
+    for (int s : c->buckets[b].systems)
+      if (c->sys[s].active) {
+        on[b] = 1;
+        break;
+      }
+  return on;
+}
 
 // Brick shapes of the spatial sort the tuner chooses from (log2 edges x | y<<4 | z<<8, bit 12 =
 // Morton order of the bricks); the first is the default.

@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
                                              int integrate) {
   const int s = cta_sys[blockIdx.x];
   const SysDev& sd = sysd[s];
+  if (!sd.active) return;  // one system per CTA; inactive systems are not gathered
   // per-CTA style table: the CTA covers one system
   __shared__ float s_scale[TILD_MAX_STYLES];
   __shared__ int s_ab[TILD_MAX_STYLES];
@@ -925,9 +926,13 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   c->launches += 2;
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
+  const std::vector<char> on = integrate ? tild_buckets_on(c) : std::vector<char>(c->buckets.size(), 1);
   if (fork(c)) return TILD_ERR_CUDA;
-  for (auto& b : c->buckets)
-    if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+  for (size_t bi = 0; bi < c->buckets.size(); bi++) {
+    const Bucket& b = c->buckets[bi];
+    if (on[bi] && tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C"))
+      return TILD_ERR_CUDA;
+  }
   if (join(c)) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_KMUL);
   if (c->D == 3) launch_kmul<3>(c, integrate);
@@ -936,9 +941,11 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (tild_check(c, cudaGetLastError(), "kmul")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_C2R);
   if (fork(c)) return TILD_ERR_CUDA;
-  for (auto& b : c->buckets)
-    if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+  for (size_t bi = 0; bi < c->buckets.size(); bi++) {
+    const Bucket& b = c->buckets[bi];
+    if (on[bi] && tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
       return TILD_ERR_CUDA;
+  }
   if (join(c)) return TILD_ERR_CUDA;
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
   for (const FieldK& fk : c->fields) {
