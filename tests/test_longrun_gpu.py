@@ -2,7 +2,8 @@
 program (its cuRAND XORWOW noise) and by the drop-in driver (Philox noise) for thousands of steps.
 The noise streams are independent, so the trajectories differ, but the equilibrium averages must
 agree: the mean potential and bond energies over the second half within statistical error (block
-averages of the logged values), and the peak of the radially averaged avg_sk at the same |k|."""
+averages of the logged values), and the radially averaged avg_sk peak: its |S|-weighted centre
+within 0.75 of a shell (shells of 0.2 in |k|) and its weight within 15 %."""
 import os
 import subprocess
 
@@ -36,13 +37,20 @@ def mean_and_error(v, blocks=6):
     return v.mean(), b.std(ddof=1) / np.sqrt(blocks)
 
 
-def sk_peak(path):
+def sk_profile(path, kmax=4.0, nbins=20):
+    """Radial average of |S(k)| over shells of |k| (avg_sk_%d.dat columns: k, |S|, |k|, Re, Im)."""
     a = np.loadtxt(path)
-    k, s = a[:, 4], a[:, 3]          # |k|, |S(k)| as avg_sk_%d.dat writes them
-    edges = np.linspace(0.0, k.max(), 41)
+    k, s = a[:, 4], a[:, 3]
+    edges = np.linspace(0.0, kmax, nbins + 1)
     idx = np.digitize(k, edges)
-    prof = np.array([s[idx == i].mean() if np.any(idx == i) else 0.0 for i in range(1, len(edges))])
-    return int(np.argmax(prof))
+    return np.array([s[idx == i].mean() if np.any(idx == i) else 0.0 for i in range(1, nbins + 1)])
+
+
+def peak_centroid(prof, last=13):
+    """|S(k)|-weighted mean shell index over the correlation-hole peak (shells below `last`):
+    steadier than the arg-max of a broad, noisy peak."""
+    i = np.arange(last)
+    return float((i * prof[:last]).sum() / prof[:last].sum())
 
 
 @pytest.mark.skipif(not os.path.exists(REF), reason="reference build not present")
@@ -65,5 +73,10 @@ def test_equilibrium_averages_match_reference_build(tmp_path):
         tol = N_SIGMA * np.hypot(sr, so) + 1e-6 * abs(mr)
         print(f"{what}: reference {mr:.6g} +- {sr:.2g}, ours {mo:.6g} +- {so:.2g}")
         assert abs(mr - mo) <= tol, what
-    pr, po = sk_peak(dirs["ref"] / "avg_sk_0.dat"), sk_peak(dirs["ours"] / "avg_sk_0.dat")
-    assert abs(pr - po) <= 1, (pr, po)
+    sr, so = sk_profile(dirs["ref"] / "avg_sk_0.dat"), sk_profile(dirs["ours"] / "avg_sk_0.dat")
+    print("S(k) shells, reference:", np.array2string(sr, precision=1))
+    print("S(k) shells, ours:     ", np.array2string(so, precision=1))
+    pr, po = peak_centroid(sr), peak_centroid(so)
+    print(f"S(k) peak centroid (shells of 0.2): reference {pr:.2f}, ours {po:.2f}")
+    assert abs(pr - po) <= 0.75, (pr, po)
+    assert abs(sr[:13].sum() - so[:13].sum()) <= 0.15 * sr[:13].sum()
