@@ -814,11 +814,12 @@ void launch_spread(tild_ctx* c) {
     k_spread_direct<D, P><<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
                                                                    c->rho_fx, c->d_status);
   } else if constexpr (P >= 2) {
-    static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
-    if (!(attr_devices >> (c->device & 63) & 1ull)) {
+    static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_devices.load() & bit)) {
       cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(int) * 12288));
-      attr_devices |= 1ull << (c->device & 63);
+      attr_devices.fetch_or(bit);
     }
     const size_t smem = sizeof(int) * (size_t)c->spread_cap;
     k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead,
@@ -829,11 +830,12 @@ void launch_spread(tild_ctx* c) {
 template <int D, int P, bool I, bool X>
 void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
   if (P >= 2 && c->gather_mode == TILD_GATHER_BOX && c->field_layout == TILD_FIELD_LINEAR) {
-    static unsigned long long attr_devices = 0;  // one bit per device that has the attribute set
-    if (!(attr_devices >> (c->device & 63) & 1ull)) {
+    static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_devices.load() & bit)) {
       cudaFuncSetAttribute(k_gather_box<D, P, I, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(float4) * kGatherBoxMax));
-      attr_devices |= 1ull << (c->device & 63);
+      attr_devices.fetch_or(bit);
     }
     k_gather_box<D, P, I, X><<<c->n_cta_bead, kTile, sizeof(float4) * (size_t)c->gather_cap, c->stream>>>(
         c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,

@@ -81,3 +81,12 @@ def test_batch_autotune_streams():
         plain = [B.get_state(i)[0] for i in range(3)]
     for a, b in zip(tuned, plain):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("brick", [0x1033, 0x1014])
+def test_2d_sort_bricks_give_the_same_trajectory(brick):
+    s = small_diblock(2, 2, nx=(32, 28), box=(16.0, 14.0), n_chains=150, N=10, seed=61)
+    ref = run(s)
+    got = run(s, {"sort_brick": brick, "sort_interval": 8})
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
