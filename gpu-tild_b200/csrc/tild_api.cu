@@ -428,10 +428,17 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   for (int s = 0; s < nsys; s++) {
     const SysHost& h = c->sys[s];
     for (int k = 0; k < h.ns_pad / kTile; k++) tb.push_back(s);
-    bspec[s] = (int)tspec.size();
-    for (long long k = 0; k < (h.g.Mh + 255) / 256; k++) tspec.push_back(s);
     bgrid[s] = (int)tgrid.size();
     for (long long k = 0; k < (h.g.M + 255) / 256; k++) tgrid.push_back(s);
+  }
+  // spectrum blocks in grid-shape order, so that each shape's blocks form one range
+  for (Bucket& b : c->buckets) {
+    b.cta_spec0 = (int)tspec.size();
+    for (int s : b.systems) {
+      bspec[s] = (int)tspec.size();
+      for (long long k = 0; k < (c->sys[s].g.Mh + 255) / 256; k++) tspec.push_back(s);
+    }
+    b.n_cta_spec = (int)tspec.size() - b.cta_spec0;
   }
   c->n_cta_bead = (int)tb.size();
   c->n_cta_spec = (int)tspec.size();
@@ -931,6 +938,7 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
   t->gather_cap = c->gather_cap;
   t->sort_brick = c->sort_brick;
   t->field_layout = c->field_layout;
+  t->fft_pipeline = c->fft_pipeline;
   t->ms_per_step = 0.0;
 }
 
@@ -954,6 +962,7 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
   c->gather_mode = t->gather_mode;
   c->gather_cap = t->gather_cap;
   c->field_layout = t->field_layout;
+  c->fft_pipeline = t->fft_pipeline != 0;
   if (t->sort_brick != c->sort_brick) {
     c->sort_brick = t->sort_brick;
     c->steps_since_sort = c->sort_interval;  // re-sort with the new keys at the next step
@@ -1059,12 +1068,18 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
       t.sort_interval = si;
       if (si != cur.sort_interval) consider(t);
     }
-  if (!c->aux.empty())
+  if (!c->aux.empty()) {
     for (int l : {0, 2, 4, 8}) {
       tild_tune t = cur;
       t.fft_streams = std::min<int>(l, (int)c->aux.size());
       if (t.fft_streams != cur.fft_streams) consider(t);
     }
+    for (int pl : {0, 1}) {
+      tild_tune t = cur;
+      t.fft_pipeline = pl;
+      if (pl != cur.fft_pipeline) consider(t);
+    }
+  }
   const int rc_trials = rc;
   // keep the fastest, then put every system back where it was
   rc = set_tune(c, &cur);

@@ -109,6 +109,7 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
   int channels = 0;
   cufftHandle r2c = 0, c2r = 0;
   bool planned = false;
+  int cta_spec0 = 0, n_cta_spec = 0;     // the shape's range of spectrum blocks (k-space multiply)
   int lane = 0;                          // auxiliary stream index (-1: main stream)
 };
 
@@ -126,6 +127,7 @@ struct tild_ctx {
   int gather_cap = 2048;                 // float4 nodes of a gather box buffer, 1024..3072
   int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
   int field_layout = TILD_FIELD_LINEAR;  // node order of the float4 force field g4
+  bool fft_pipeline = false;             // per shape on its stream: convert, R2C, multiply, C2R
   long long g4_total = 0;
   int D = 3, P = 1;
   int nsys = 1;
@@ -394,6 +396,7 @@ __host__ __device__ inline float ramp_ratio(const SysDev& d, int k, long long st
 // ---- host-side entry points between translation units ------------------------------------
 int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);

@@ -309,8 +309,9 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
                                              const float* __restrict__ utab_all, const float* __restrict__ ctab_all,
                                              const float* __restrict__ kd_all, const int* __restrict__ cta_sys,
                                              const int* __restrict__ blk0, const SysDev* __restrict__ sysd,
-                                             int integrate) {
-  const int s = cta_sys[blockIdx.x];
+                                             int integrate, int blk_off) {
+  const int blk = blockIdx.x + blk_off;
+  const int s = cta_sys[blk];
   const SysDev& sd = sysd[s];
   if (!sd.active) return;  // one system per CTA; inactive systems are not gathered
   // per-CTA style table: the CTA covers one system
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   if (threadIdx.x == 0) s_nfft = sd.nfft;
   __syncthreads();
   const Geom& g = sd.g;
-  const long long h = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
+  const long long h = (long long)(blk - blk0[s]) * blockDim.x + threadIdx.x;
   const long long Mh = g.Mh;
   if (h >= Mh) return;
   const int T = sd.T, C = sd.C;
@@ -880,18 +881,21 @@ void dispatch_p_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
   }
 }
 
+// k-space multiply over spectrum blocks [off, off + n) (all of them by default) on stream st
 template <int D>
-void launch_kmul(tild_ctx* c, bool integ) {
+void launch_kmul(tild_ctx* c, bool integ, cudaStream_t st = nullptr, int off = 0, int n = -1) {
   const float2* rk = reinterpret_cast<const float2*>(c->rhok);
   float2* gk = reinterpret_cast<float2*>(c->gk);
   int* blk0 = c->cta_spec + c->n_cta_spec;  // first-block table stored after the lookup table
-  const int n = c->n_cta_spec;
+  if (n < 0) n = c->n_cta_spec;
+  if (!st) st = c->stream;
+  if (n == 0) return;
   switch (c->maxT) {
-    case 1: k_kmul<D, 1><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
-    case 2: k_kmul<D, 2><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
-    case 3: k_kmul<D, 3><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
-    case 4: k_kmul<D, 4><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
-    default: k_kmul<D, 0><<<n, 256, 0, c->stream>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ); break;
+    case 1: k_kmul<D, 1><<<n, 256, 0, st>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ, off); break;
+    case 2: k_kmul<D, 2><<<n, 256, 0, st>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ, off); break;
+    case 3: k_kmul<D, 3><<<n, 256, 0, st>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ, off); break;
+    case 4: k_kmul<D, 4><<<n, 256, 0, st>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ, off); break;
+    default: k_kmul<D, 0><<<n, 256, 0, st>>>(rk, gk, c->utab, c->ctab, c->kd, c->cta_spec, blk0, c->d_sys, integ, off); break;
   }
 }
 
@@ -923,12 +927,36 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   tild_mark(c, STAGE_SPREAD);
   if (c->D == 3) dispatch_p_spread<3>(c);
   else dispatch_p_spread<2>(c);
+  c->launches++;
+  const std::vector<char> on = integrate ? tild_buckets_on(c) : std::vector<char>(c->buckets.size(), 1);
+  if (c->fft_pipeline && c->lanes > 0) {
+    // each grid shape runs conversion, R2C, k-space multiply and C2R in order on its stream, so
+    // one shape's transforms overlap another's element-wise passes (one profiling stage)
+    tild_mark(c, STAGE_R2C);
+    if (fork(c)) return TILD_ERR_CUDA;
+    for (size_t bi = 0; bi < c->buckets.size(); bi++) {
+      const Bucket& b = c->buckets[bi];
+      cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
+      const long long n = (long long)b.channels * b.nx[0] * b.nx[1] * b.nx[2];
+      k_fix_to_float<<<nblk(n, 256), 256, 0, bs>>>(c->rho_fx + b.grid0, c->rho + b.grid0, n);
+      c->launches++;
+      if (!on[bi]) continue;
+      if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+      if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
+      else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
+      c->launches++;
+      if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+        return TILD_ERR_CUDA;
+    }
+    if (join(c)) return TILD_ERR_CUDA;
+    if (tild_check(c, cudaGetLastError(), "shape pipeline")) return TILD_ERR_CUDA;
+    return tild_finish_forces(c, integrate, f_bead, f_sys);
+  }
   tild_mark(c, STAGE_ZERO);
   k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
-  c->launches += 2;
+  c->launches++;
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
-  const std::vector<char> on = integrate ? tild_buckets_on(c) : std::vector<char>(c->buckets.size(), 1);
   if (fork(c)) return TILD_ERR_CUDA;
   for (size_t bi = 0; bi < c->buckets.size(); bi++) {
     const Bucket& b = c->buckets[bi];
@@ -949,6 +977,11 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       return TILD_ERR_CUDA;
   }
   if (join(c)) return TILD_ERR_CUDA;
+  return tild_finish_forces(c, integrate, f_bead, f_sys);
+}
+
+// fieldphase, interleave, gather (+ bonds + integrators) and the step tail
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
   for (const FieldK& fk : c->fields) {
     const SysHost& h = c->sys[fk.sys];

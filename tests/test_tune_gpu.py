@@ -70,6 +70,9 @@ def test_batch_autotune_streams():
         before = [B.get_state(i) for i in range(3)]
         best = B.autotune(trial_steps=32)
         assert 0 <= best["fft_streams"] <= 8
+        t = B.get_tune()
+        t.fft_streams, t.fft_pipeline = 2, 1     # the per-shape pipeline must not change results
+        B.set_tune(t)
         for i in range(3):
             assert B.step_count(i) == 0
             for a, b in zip(before[i], B.get_state(i)):
