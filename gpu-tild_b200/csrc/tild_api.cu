@@ -428,17 +428,19 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   for (int s = 0; s < nsys; s++) {
     const SysHost& h = c->sys[s];
     for (int k = 0; k < h.ns_pad / kTile; k++) tb.push_back(s);
-    bgrid[s] = (int)tgrid.size();
-    for (long long k = 0; k < (h.g.M + 255) / 256; k++) tgrid.push_back(s);
   }
-  // spectrum blocks in grid-shape order, so that each shape's blocks form one range
+  // spectrum and grid blocks in grid-shape order, so that each shape's blocks form one range
   for (Bucket& b : c->buckets) {
     b.cta_spec0 = (int)tspec.size();
+    b.cta_grid0 = (int)tgrid.size();
     for (int s : b.systems) {
       bspec[s] = (int)tspec.size();
       for (long long k = 0; k < (c->sys[s].g.Mh + 255) / 256; k++) tspec.push_back(s);
+      bgrid[s] = (int)tgrid.size();
+      for (long long k = 0; k < (c->sys[s].g.M + 255) / 256; k++) tgrid.push_back(s);
     }
     b.n_cta_spec = (int)tspec.size() - b.cta_spec0;
+    b.n_cta_grid = (int)tgrid.size() - b.cta_grid0;
   }
   c->n_cta_bead = (int)tb.size();
   c->n_cta_spec = (int)tspec.size();

@@ -110,6 +110,7 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
   cufftHandle r2c = 0, c2r = 0;
   bool planned = false;
   int cta_spec0 = 0, n_cta_spec = 0;     // the shape's range of spectrum blocks (k-space multiply)
+  int cta_grid0 = 0, n_cta_grid = 0;     // and of grid blocks (interleave)
   int lane = 0;                          // auxiliary stream index (-1: main stream)
 };
 
@@ -396,7 +397,7 @@ __host__ __device__ inline float ramp_ratio(const SysDev& d, int k, long long st
 // ---- host-side entry points between translation units ------------------------------------
 int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
-int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved);
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);

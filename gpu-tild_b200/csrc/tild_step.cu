@@ -417,13 +417,14 @@ __global__ void k_fieldphase_apply(float* __restrict__ gfield, const float* __re
 template <int D>
 __global__ void k_interleave(const float* __restrict__ planar_all, float4* __restrict__ g4_all,
                              const int* __restrict__ cta_sys, const int* __restrict__ blk0,
-                             const SysDev* __restrict__ sysd, int layout) {
-  const int s = cta_sys[blockIdx.x];
+                             const SysDev* __restrict__ sysd, int layout, int blk_off) {
+  const int blk = blockIdx.x + blk_off;
+  const int s = cta_sys[blk];
   const SysDev& sd = sysd[s];
   if (!sd.active) return;  // inactive systems are not gathered
   const Geom& g = sd.g;
   const long long M = g.M;
-  const long long m = (long long)(blockIdx.x - blk0[s]) * blockDim.x + threadIdx.x;
+  const long long m = (long long)(blk - blk0[s]) * blockDim.x + threadIdx.x;
   if (m >= M) return;
   long long dst = m;
   if (layout != TILD_FIELD_LINEAR) {
@@ -881,6 +882,16 @@ void dispatch_p_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
   }
 }
 
+// interleave over grid blocks [off, off + n) on stream st
+void launch_interleave(tild_ctx* c, cudaStream_t st, int off, int n) {
+  if (n == 0) return;
+  int* blk0 = c->cta_grid + c->n_cta_grid;
+  if (c->D == 3)
+    k_interleave<3><<<n, 256, 0, st>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout, off);
+  else
+    k_interleave<2><<<n, 256, 0, st>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout, off);
+}
+
 // k-space multiply over spectrum blocks [off, off + n) (all of them by default) on stream st
 template <int D>
 void launch_kmul(tild_ctx* c, bool integ, cudaStream_t st = nullptr, int off = 0, int n = -1) {
@@ -947,10 +958,14 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       c->launches++;
       if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
         return TILD_ERR_CUDA;
+      if (c->fields.empty()) {  // fieldphase edits the planar fields first when present
+        launch_interleave(c, bs, b.cta_grid0, b.n_cta_grid);
+        c->launches++;
+      }
     }
     if (join(c)) return TILD_ERR_CUDA;
     if (tild_check(c, cudaGetLastError(), "shape pipeline")) return TILD_ERR_CUDA;
-    return tild_finish_forces(c, integrate, f_bead, f_sys);
+    return tild_finish_forces(c, integrate, f_bead, f_sys, c->fields.empty());
   }
   tild_mark(c, STAGE_ZERO);
   k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
@@ -977,11 +992,12 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       return TILD_ERR_CUDA;
   }
   if (join(c)) return TILD_ERR_CUDA;
-  return tild_finish_forces(c, integrate, f_bead, f_sys);
+  return tild_finish_forces(c, integrate, f_bead, f_sys, false);
 }
 
-// fieldphase, interleave, gather (+ bonds + integrators) and the step tail
-int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
+// fieldphase, interleave (unless the shape pipeline did it), gather (+ bonds + integrators) and
+// the step tail
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved) {
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
   for (const FieldK& fk : c->fields) {
     const SysHost& h = c->sys[fk.sys];
@@ -991,12 +1007,10 @@ int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   }
   tild_mark(c, STAGE_INTERLEAVE);
   {
-    int* blk0 = c->cta_grid + c->n_cta_grid;
-    if (c->D == 3)
-      k_interleave<3><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout);
-    else
-      k_interleave<2><<<c->n_cta_grid, 256, 0, c->stream>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout);
-    c->launches++;
+    if (!interleaved) {
+      launch_interleave(c, c->stream, 0, c->n_cta_grid);
+      c->launches++;
+    }
   }
   tild_mark(c, STAGE_GATHER);
   if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys);
