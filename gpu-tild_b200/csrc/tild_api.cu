@@ -345,10 +345,6 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
     const Geom& g = h.g;
     h.cap = capacity ? std::max(h.ns, (int)capacity[s]) : h.ns;
     h.ns_pad = (h.cap + kTile - 1) / kTile * kTile;
-    h.slot0 = (int)slots;
-    h.bead0 = (int)beads;
-    slots += h.ns_pad;
-    beads += h.cap;
     for (int i = 0; i < cfg.n_styles; i++)
       if (cfg.styles[i].style == TILD_STYLE_FIELDPHASE) {
         FieldK f;
@@ -383,11 +379,9 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
     }
     c->buckets[bi].systems.push_back(s);
     h.bucket = bi;
-    // layout part of the device descriptor
+    // layout part of the device descriptor (slots are placed below, shape by shape)
     SysDev& d = c->h_sys[s];
-    d.slot0 = h.slot0;
     d.ns_pad = h.ns_pad;
-    d.bead0 = h.bead0;
     d.active = 1;
     d.utab0 = h.utab0;
     d.ctab0 = h.ctab0;
@@ -398,12 +392,21 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   // channel layout: bucket by bucket so each bucket is one batched transform
   long long grid = 0, spec = 0;
   long long g4tot = 0;
+  int rank = 0;
   for (Bucket& b : c->buckets) {
     b.grid0 = grid;
     b.spec0 = spec;
     b.channels = 0;
     for (int s : b.systems) {
       SysHost& h = c->sys[s];
+      // slots shape by shape too, so that a shape's beads are one range of particle blocks
+      h.slot0 = (int)slots;
+      h.bead0 = (int)beads;
+      slots += h.ns_pad;
+      beads += h.cap;
+      c->h_sys[s].slot0 = h.slot0;
+      c->h_sys[s].bead0 = h.bead0;
+      c->h_sys[s].slot_rank = rank++;
       h.grid0 = grid;
       h.spec0 = spec;
       h.Mb = tild_field_stride(h.g, h.D);
@@ -425,20 +428,19 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   c->nbeads = (int)beads;
   // CTA -> system lookup tables (grid and spectrum tables carry each system's first block after them)
   std::vector<int> tb, tspec, tgrid, bspec(nsys), bgrid(nsys);
-  for (int s = 0; s < nsys; s++) {
-    const SysHost& h = c->sys[s];
-    for (int k = 0; k < h.ns_pad / kTile; k++) tb.push_back(s);
-  }
-  // spectrum and grid blocks in grid-shape order, so that each shape's blocks form one range
+  // particle, spectrum and grid blocks in grid-shape order, so each shape's blocks form one range
   for (Bucket& b : c->buckets) {
+    b.cta_bead0 = (int)tb.size();
     b.cta_spec0 = (int)tspec.size();
     b.cta_grid0 = (int)tgrid.size();
     for (int s : b.systems) {
+      for (int k = 0; k < c->sys[s].ns_pad / kTile; k++) tb.push_back(s);
       bspec[s] = (int)tspec.size();
       for (long long k = 0; k < (c->sys[s].g.Mh + 255) / 256; k++) tspec.push_back(s);
       bgrid[s] = (int)tgrid.size();
       for (long long k = 0; k < (c->sys[s].g.M + 255) / 256; k++) tgrid.push_back(s);
     }
+    b.n_cta_bead = (int)tb.size() - b.cta_bead0;
     b.n_cta_spec = (int)tspec.size() - b.cta_spec0;
     b.n_cta_grid = (int)tgrid.size() - b.cta_grid0;
   }
@@ -949,7 +951,7 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
       t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
       t->gather_mode < TILD_GATHER_DIRECT || t->gather_mode > TILD_GATHER_BOX || t->gather_cap < 1024 ||
       t->gather_cap > 3072 || t->field_layout < TILD_FIELD_LINEAR || t->field_layout > TILD_FIELD_BRICK ||
-      (t->field_layout == TILD_FIELD_BRICK && c->D != 3))
+      (t->field_layout == TILD_FIELD_BRICK && c->D != 3) || t->fft_pipeline < 0 || t->fft_pipeline > 2)
     return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
   if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
   {
@@ -964,7 +966,7 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
   c->gather_mode = t->gather_mode;
   c->gather_cap = t->gather_cap;
   c->field_layout = t->field_layout;
-  c->fft_pipeline = t->fft_pipeline != 0;
+  c->fft_pipeline = t->fft_pipeline;
   if (t->sort_brick != c->sort_brick) {
     c->sort_brick = t->sort_brick;
     c->steps_since_sort = c->sort_interval;  // re-sort with the new keys at the next step
@@ -1076,7 +1078,7 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
       t.fft_streams = std::min<int>(l, (int)c->aux.size());
       if (t.fft_streams != cur.fft_streams) consider(t);
     }
-    for (int pl : {0, 1}) {
+    for (int pl : {0, 1, 2}) {
       tild_tune t = cur;
       t.fft_pipeline = pl;
       if (pl != cur.fft_pipeline) consider(t);

@@ -57,6 +57,7 @@ struct SysDev {
   Geom g;
   int T, C, kbits, nfft;
   int slot0, ns, ns_pad, bead0;
+  int slot_rank;                   // position of the system's slot range (the sort keeps the ranges)
   int active;                      // 0: skipped by the particle kernels
   long long grid0;                 // channel 0 of this system in rho / rho_fx / g4 (grid points)
   long long spec0;                 // channel 0 in rhok (half-spectrum points)
@@ -111,6 +112,7 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R p
   bool planned = false;
   int cta_spec0 = 0, n_cta_spec = 0;     // the shape's range of spectrum blocks (k-space multiply)
   int cta_grid0 = 0, n_cta_grid = 0;     // and of grid blocks (interleave)
+  int cta_bead0 = 0, n_cta_bead = 0;     // and of particle blocks (spread, gather)
   int lane = 0;                          // auxiliary stream index (-1: main stream)
 };
 
@@ -128,7 +130,7 @@ struct tild_ctx {
   int gather_cap = 2048;                 // float4 nodes of a gather box buffer, 1024..3072
   int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
   int field_layout = TILD_FIELD_LINEAR;  // node order of the float4 force field g4
-  bool fft_pipeline = false;             // per shape on its stream: convert, R2C, multiply, C2R
+  int fft_pipeline = 0;                  // per shape on its stream: 1 the grid stages, 2 the whole step
   long long g4_total = 0;
   int D = 3, P = 1;
   int nsys = 1;
@@ -397,7 +399,7 @@ __host__ __device__ inline float ramp_ratio(const SysDev& d, int k, long long st
 // ---- host-side entry points between translation units ------------------------------------
 int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
-int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved);
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved, bool gathered);
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);

@@ -3,9 +3,9 @@
 // The reference keeps beads in file order for its whole run (d_x, device_comm_utils.cu:5-17), so
 // every stencil access of its spread and gather lands on an unrelated cache line.  Here the slots
 // are re-sorted every `sort_interval` steps by the grid cell of the bead, cells taken in 4x4x4
-// bricks (8x8 in 2D) so that a warp's beads share stencil nodes.  The key carries the system in
-// its high bits and padding slots get the largest cell code, so each system keeps its slot range
-// with its beads first.  The sort is stable (CUB radix sort on (key, slot)); every per-bead array
+// bricks (8x8 in 2D) so that a warp's beads share stencil nodes.  The key carries the rank of the
+// system's slot range in its high bits and padding slots get the largest cell code, so each
+// system keeps its slot range with its beads first.  The sort is stable (CUB radix sort on (key, slot)); every per-bead array
 // is permuted and bond partners are renumbered, so the physics never depends on the order: noise
 // is keyed by the bead id, and outputs are written by bead id.
 #include "tild_internal.cuh"
@@ -59,7 +59,7 @@ __global__ void k_sort_keys(const float4* __restrict__ pos, const int* __restric
                            ((unsigned)c[0] & ((1u << sh[0]) - 1));
     cell = (bidx << (sh[0] + sh[1] + sh[2])) | local;
   }
-  keys[slot] = ((unsigned)sys << cell_bits) | cell;
+  keys[slot] = ((unsigned)sysd[sys].slot_rank << cell_bits) | cell;
   vals[slot] = slot;
 }
 

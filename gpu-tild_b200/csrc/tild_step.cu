@@ -123,15 +123,16 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
                                                      const int* __restrict__ cta_sys,
                                                      const SysDev* __restrict__ sysd,
                                                      unsigned long long* __restrict__ rho_fx_all, int cap,
-                                                     int* status) {
+                                                     int* status, int blk_off) {
   extern __shared__ int smi[];
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ long long s_row[kMaxRows];
-  const SysDev& sd = sysd[cta_sys[blockIdx.x]];  // inactive systems too (see k_fix_to_float)
+  const int blk = blockIdx.x + blk_off;
+  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
   const Geom g = sd.g;
   const int T = sd.T, C = sd.C, kbits = sd.kbits;
   unsigned long long* rho_fx = rho_fx_all + sd.grid0;
-  const int i0 = blockIdx.x * blockDim.x;
+  const int i0 = blk * blockDim.x;
   const int i = i0 + threadIdx.x;
   chunk_origin<D, P>(pos, i0, g, s_g0, s_min, s_max);
   float W[3][P + 1];
@@ -243,9 +244,11 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
 template <int D, int P>
 __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict__ pos, const float* __restrict__ charge,
                                                       const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd,
-                                                      unsigned long long* __restrict__ rho_fx_all, int* status) {
-  const SysDev& sd = sysd[cta_sys[blockIdx.x]];  // inactive systems too (see k_fix_to_float)
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                      unsigned long long* __restrict__ rho_fx_all, int* status,
+                                                      int blk_off) {
+  const int blk = blockIdx.x + blk_off;
+  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
+  const int i = blk * blockDim.x + threadIdx.x;
   const float4 p = pos[i];
   const int t = tild_type_of(p.w);
   if (t == kPadType) return;
@@ -583,10 +586,10 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 :
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
     const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
-    int layout, int* status) {
-  const int s = cta_sys[blockIdx.x];
+    int layout, int* status, int blk_off) {
+  const int s = cta_sys[blockIdx.x + blk_off];
   const SysDev& sd = sysd[s];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (blockIdx.x + blk_off) * blockDim.x + threadIdx.x;
   if (!sd.active) {
     if (INTEG) pos_io[i] = pos_in[i];  // inactive systems keep x_n through the buffer rotation
     return;
@@ -677,13 +680,13 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
     const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
-    int box_cap, int* status) {
+    int box_cap, int* status, int blk_off) {
   extern __shared__ float4 sbox[];
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ int s_row[kMaxRows];
-  const int s = cta_sys[blockIdx.x];
+  const int s = cta_sys[blockIdx.x + blk_off];
   const SysDev& sd = sysd[s];
-  const int i0 = blockIdx.x * blockDim.x;
+  const int i0 = (blockIdx.x + blk_off) * blockDim.x;
   const int i = i0 + threadIdx.x;
   if (!sd.active) {  // one system per CTA: every thread leaves here together
     if (INTEG) pos_io[i] = pos_in[i];
@@ -810,11 +813,19 @@ __global__ void k_advance_steps(SysDev* __restrict__ sysd, int nsys) {
 // Order <= 1 always spreads directly; order >= 2 uses the shared box unless the tuner chose the
 // direct kernel.  The box (spread_cap words, at most 12288 = 48 KB) plus the kernel's static
 // shared memory exceeds the default 48 KB, so the opt-in limit is raised once per device.
+// particle blocks [off, off + n) on stream st (a grid shape's range in the shape pipeline)
+struct BeadRange {
+  cudaStream_t st;
+  int off, n;
+};
+inline BeadRange all_beads(tild_ctx* c) { return {c->stream, 0, c->n_cta_bead}; }
+
 template <int D, int P>
-void launch_spread(tild_ctx* c) {
+void launch_spread(tild_ctx* c, BeadRange r) {
+  if (r.n == 0) return;
   if (P <= 1 || c->spread_mode == TILD_SPREAD_DIRECT) {
-    k_spread_direct<D, P><<<c->n_cta_bead, kTile, 0, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys,
-                                                                   c->rho_fx, c->d_status);
+    k_spread_direct<D, P><<<r.n, kTile, 0, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
+                                                    c->d_status, r.off);
   } else if constexpr (P >= 2) {
     static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
     const unsigned long long bit = 1ull << (c->device & 63);
@@ -824,13 +835,14 @@ void launch_spread(tild_ctx* c) {
       attr_devices.fetch_or(bit);
     }
     const size_t smem = sizeof(int) * (size_t)c->spread_cap;
-    k_spread_tiled<D, P><<<c->n_cta_bead, kTile, smem, c->stream>>>(c->pos[c->cur], c->charge, c->cta_bead,
-                                                                     c->d_sys, c->rho_fx, c->spread_cap, c->d_status);
+    k_spread_tiled<D, P><<<r.n, kTile, smem, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
+                                                      c->spread_cap, c->d_status, r.off);
   }
 }
 
 template <int D, int P, bool I, bool X>
-void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
+void launch_gather_k(tild_ctx* c, float* f_out, int f_sys, BeadRange r) {
+  if (r.n == 0) return;
   if (P >= 2 && c->gather_mode == TILD_GATHER_BOX && c->field_layout == TILD_FIELD_LINEAR) {
     static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
     const unsigned long long bit = 1ull << (c->device & 63);
@@ -839,46 +851,46 @@ void launch_gather_k(tild_ctx* c, float* f_out, int f_sys) {
                            (int)(sizeof(float4) * kGatherBoxMax));
       attr_devices.fetch_or(bit);
     }
-    k_gather_box<D, P, I, X><<<c->n_cta_bead, kTile, sizeof(float4) * (size_t)c->gather_cap, c->stream>>>(
+    k_gather_box<D, P, I, X><<<r.n, kTile, sizeof(float4) * (size_t)c->gather_cap, r.st>>>(
         c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
-        c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->gather_cap, c->d_status);
+        c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->gather_cap, c->d_status, r.off);
     return;
   }
-  k_gather<D, P, I, X><<<c->n_cta_bead, kTile, 0, c->stream>>>(
+  k_gather<D, P, I, X><<<r.n, kTile, 0, r.st>>>(
       c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
-      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->d_status);
+      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->d_status, r.off);
 }
 
 template <int D, int P>
-void launch_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
+void launch_gather(tild_ctx* c, bool integ, float* f_out, int f_sys, BeadRange r) {
   const bool xw = c->rng == TILD_RNG_XORWOW;
   if (integ) {
-    if (xw) launch_gather_k<D, P, true, true>(c, f_out, f_sys);
-    else launch_gather_k<D, P, true, false>(c, f_out, f_sys);
+    if (xw) launch_gather_k<D, P, true, true>(c, f_out, f_sys, r);
+    else launch_gather_k<D, P, true, false>(c, f_out, f_sys, r);
   } else {
-    launch_gather_k<D, P, false, false>(c, f_out, f_sys);
+    launch_gather_k<D, P, false, false>(c, f_out, f_sys, r);
   }
 }
 
 template <int D>
-void dispatch_p_spread(tild_ctx* c) {
+void dispatch_p_spread(tild_ctx* c, BeadRange r) {
   switch (c->P) {
-    case 0: launch_spread<D, 0>(c); break;
-    case 1: launch_spread<D, 1>(c); break;
-    case 2: launch_spread<D, 2>(c); break;
-    case 3: launch_spread<D, 3>(c); break;
-    default: launch_spread<D, 4>(c); break;
+    case 0: launch_spread<D, 0>(c, r); break;
+    case 1: launch_spread<D, 1>(c, r); break;
+    case 2: launch_spread<D, 2>(c, r); break;
+    case 3: launch_spread<D, 3>(c, r); break;
+    default: launch_spread<D, 4>(c, r); break;
   }
 }
 
 template <int D>
-void dispatch_p_gather(tild_ctx* c, bool integ, float* f_out, int f_sys) {
+void dispatch_p_gather(tild_ctx* c, bool integ, float* f_out, int f_sys, BeadRange r) {
   switch (c->P) {
-    case 0: launch_gather<D, 0>(c, integ, f_out, f_sys); break;
-    case 1: launch_gather<D, 1>(c, integ, f_out, f_sys); break;
-    case 2: launch_gather<D, 2>(c, integ, f_out, f_sys); break;
-    case 3: launch_gather<D, 3>(c, integ, f_out, f_sys); break;
-    default: launch_gather<D, 4>(c, integ, f_out, f_sys); break;
+    case 0: launch_gather<D, 0>(c, integ, f_out, f_sys, r); break;
+    case 1: launch_gather<D, 1>(c, integ, f_out, f_sys, r); break;
+    case 2: launch_gather<D, 2>(c, integ, f_out, f_sys, r); break;
+    case 3: launch_gather<D, 3>(c, integ, f_out, f_sys, r); break;
+    default: launch_gather<D, 4>(c, integ, f_out, f_sys, r); break;
   }
 }
 
@@ -935,12 +947,45 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
     int rs = tild_sort_beads(c);
     if (rs) return rs;
   }
-  tild_mark(c, STAGE_SPREAD);
-  if (c->D == 3) dispatch_p_spread<3>(c);
-  else dispatch_p_spread<2>(c);
-  c->launches++;
   const std::vector<char> on = integrate ? tild_buckets_on(c) : std::vector<char>(c->buckets.size(), 1);
-  if (c->fft_pipeline && c->lanes > 0) {
+  if (c->fft_pipeline >= 2 && c->lanes > 0 && c->fields.empty()) {
+    // each grid shape runs its whole step in order on its stream: spread, conversion, R2C,
+    // k-space multiply, C2R, interleave and gather, so one shape's transforms overlap another's
+    // particle kernels (one profiling stage).  Idle shapes still spread and gather, which keeps
+    // their densities current and their positions held.
+    tild_mark(c, STAGE_R2C);
+    if (fork(c)) return TILD_ERR_CUDA;
+    for (size_t bi = 0; bi < c->buckets.size(); bi++) {
+      const Bucket& b = c->buckets[bi];
+      cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
+      const BeadRange r{bs, b.cta_bead0, b.n_cta_bead};
+      if (c->D == 3) dispatch_p_spread<3>(c, r);
+      else dispatch_p_spread<2>(c, r);
+      const long long n = (long long)b.channels * b.nx[0] * b.nx[1] * b.nx[2];
+      k_fix_to_float<<<nblk(n, 256), 256, 0, bs>>>(c->rho_fx + b.grid0, c->rho + b.grid0, n);
+      c->launches += 2;
+      if (on[bi]) {
+        if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+        if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
+        else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
+        if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+          return TILD_ERR_CUDA;
+        launch_interleave(c, bs, b.cta_grid0, b.n_cta_grid);
+        c->launches += 2;
+      }
+      if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys, r);
+      else dispatch_p_gather<2>(c, integrate, f_bead, f_sys, r);
+      c->launches++;
+    }
+    if (join(c)) return TILD_ERR_CUDA;
+    if (tild_check(c, cudaGetLastError(), "shape pipeline")) return TILD_ERR_CUDA;
+    return tild_finish_forces(c, integrate, f_bead, f_sys, true, true);
+  }
+  tild_mark(c, STAGE_SPREAD);
+  if (c->D == 3) dispatch_p_spread<3>(c, all_beads(c));
+  else dispatch_p_spread<2>(c, all_beads(c));
+  c->launches++;
+  if (c->fft_pipeline >= 1 && c->lanes > 0) {
     // each grid shape runs conversion, R2C, k-space multiply and C2R in order on its stream, so
     // one shape's transforms overlap another's element-wise passes (one profiling stage)
     tild_mark(c, STAGE_R2C);
@@ -965,7 +1010,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
     }
     if (join(c)) return TILD_ERR_CUDA;
     if (tild_check(c, cudaGetLastError(), "shape pipeline")) return TILD_ERR_CUDA;
-    return tild_finish_forces(c, integrate, f_bead, f_sys, c->fields.empty());
+    return tild_finish_forces(c, integrate, f_bead, f_sys, c->fields.empty(), false);
   }
   tild_mark(c, STAGE_ZERO);
   k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
@@ -992,12 +1037,12 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       return TILD_ERR_CUDA;
   }
   if (join(c)) return TILD_ERR_CUDA;
-  return tild_finish_forces(c, integrate, f_bead, f_sys, false);
+  return tild_finish_forces(c, integrate, f_bead, f_sys, false, false);
 }
 
 // fieldphase, interleave (unless the shape pipeline did it), gather (+ bonds + integrators) and
 // the step tail
-int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved) {
+int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved, bool gathered) {
   if (!c->fields.empty()) tild_mark(c, STAGE_FIELD);
   for (const FieldK& fk : c->fields) {
     const SysHost& h = c->sys[fk.sys];
@@ -1005,18 +1050,18 @@ int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bo
                                                                  c->frfield + fk.fr0, fk.a, fk.b, c->D, h.g.M);
     c->launches++;
   }
-  tild_mark(c, STAGE_INTERLEAVE);
-  {
-    if (!interleaved) {
-      launch_interleave(c, c->stream, 0, c->n_cta_grid);
-      c->launches++;
-    }
+  if (!interleaved) {
+    tild_mark(c, STAGE_INTERLEAVE);
+    launch_interleave(c, c->stream, 0, c->n_cta_grid);
+    c->launches++;
   }
-  tild_mark(c, STAGE_GATHER);
-  if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys);
-  else dispatch_p_gather<2>(c, integrate, f_bead, f_sys);
-  c->launches++;
-  if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
+  if (!gathered) {
+    tild_mark(c, STAGE_GATHER);
+    if (c->D == 3) dispatch_p_gather<3>(c, integrate, f_bead, f_sys, all_beads(c));
+    else dispatch_p_gather<2>(c, integrate, f_bead, f_sys, all_beads(c));
+    c->launches++;
+    if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
+  }
   if (integrate) {
     tild_mark(c, STAGE_TAIL);
     k_advance_steps<<<nblk(c->nsys, 128), 128, 0, c->stream>>>(c->d_sys, c->nsys);

@@ -71,7 +71,7 @@ class Tune(C.Structure):
                 "spread_cap_words": self.spread_cap, "sort_interval": self.sort_interval,
                 "fft_streams": self.fft_streams, "gather_mode": ("direct", "box")[self.gather_mode],
                 "gather_cap_nodes": self.gather_cap, "sort_brick": hex(self.sort_brick),
-                "field_layout": ("linear", "brick")[self.field_layout], "fft_pipeline": bool(self.fft_pipeline),
+                "field_layout": ("linear", "brick")[self.field_layout], "fft_pipeline": int(self.fft_pipeline),
                 "ms_per_step": self.ms_per_step}
 
 

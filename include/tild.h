@@ -292,9 +292,10 @@ typedef struct tild_tune {
                              0x1033, 0x1014 */
   int32_t field_layout;   /* node order of the force field the gather reads: x-fastest (LINEAR) or 4x4x4
                              bricks of consecutive nodes (BRICK, 3D; the box gather needs LINEAR) */
-  int32_t fft_pipeline;   /* several grid shapes: 1 runs each shape's fixed-point conversion, R2C,
-                             k-space multiply and C2R in sequence on its own stream, so shapes overlap
-                             across stages; 0 runs each stage for all shapes before the next */
+  int32_t fft_pipeline;   /* several grid shapes: 0 runs each stage for all shapes before the next;
+                             1 runs each shape's fixed-point conversion, R2C, k-space multiply, C2R
+                             and interleave in sequence on its own stream; 2 runs each shape's whole
+                             step (spread to gather) on its stream (without fieldphase styles) */
   double ms_per_step;     /* tild_autotune: measured step time with these settings */
 } tild_tune;
 int32_t tild_get_tune(tild_ctx* ctx, tild_tune* out);

@@ -71,7 +71,7 @@ def test_batch_autotune_streams():
         best = B.autotune(trial_steps=32)
         assert 0 <= best["fft_streams"] <= 8
         t = B.get_tune()
-        t.fft_streams, t.fft_pipeline = 2, 1     # the per-shape pipeline must not change results
+        t.fft_streams, t.fft_pipeline = 2, 2     # the per-shape pipeline must not change results
         B.set_tune(t)
         for i in range(3):
             assert B.step_count(i) == 0
@@ -92,4 +92,21 @@ def test_2d_sort_bricks_give_the_same_trajectory(brick):
     ref = run(s)
     got = run(s, {"sort_brick": brick, "sort_interval": 8})
     for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_shape_pipeline_gives_the_same_trajectories(level):
+    systems = [small_diblock(3, 1, nx=(16, 16, 16), box=(8.0, 8.0, 8.0), seed=71),
+               small_diblock(3, 1, nx=(12, 14, 16), box=(6.0, 7.0, 8.0), n_chains=70, seed=72),
+               small_diblock(3, 1, nx=(20, 20, 20), box=(10.0, 10.0, 10.0), n_chains=200, seed=73)]
+    out = []
+    for lv in (0, level):
+        with tild.Batch(systems) as B:
+            t = B.get_tune()
+            t.fft_streams, t.fft_pipeline = 2, lv
+            B.set_tune(t)
+            B.step(70)
+            out.append([B.get_state(i)[0] for i in range(3)])
+    for a, b in zip(*out):
         assert np.array_equal(a, b)
