@@ -335,6 +335,9 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   c->sort_brick = tild_brick_candidates(cfgs[0].dim == 2 ? 2 : 3)[0];
   c->steps_since_sort = c->sort_interval;
   c->spread_cap = 12288;
+  // order <= 1 spreads by global atomics, which the gather absorbs at no cost; the order >= 2
+  // shared box costs the gather its L1 share and barriers (both measured on the B200)
+  c->spread_ahead = cfgs[0].pmeorder <= 1 ? 1 : 0;
   long long slots = 0, beads = 0, utab = 0, virk = 0, ctab = 0, kd = 0, fr = 0;
   // buckets by grid shape (order of first appearance)
   for (int s = 0; s < nsys; s++) {
@@ -542,6 +545,7 @@ int sys_set_topology(tild_ctx* c, int s, const int32_t* types, const float* char
   SysHost& h = c->sys[s];
   if (h.C && !charges) return set_err(c, TILD_ERR_BAD_INPUT, "charges required when do_charges is set");
   cudaSetDevice(c->device);
+  if (tild_drop_ahead(c)) return TILD_ERR_CUDA;
   const int ns = h.ns, np = h.ns_pad;
   std::vector<int> nbr(3 * (size_t)np, 0), info(np, 0), bid(np, -1), slot_of(ns);
   std::vector<float> q;
@@ -594,6 +598,7 @@ int sys_set_state(tild_ctx* c, int s, const float* x, const float* xo, const flo
   const size_t n = (size_t)h.ns * h.D;
   for (size_t i = 0; i < n; i++)
     if (!std::isfinite(x[i])) return set_err(c, TILD_ERR_NAN, "non-finite position in tild_set_state");
+  if (tild_drop_ahead(c)) return TILD_ERR_CUDA;
   const unsigned nb = nblk(h.ns, 256);
   cudaStream_t st = c->stream;
   const int* so = c->slot_of + h.bead0;
@@ -677,9 +682,14 @@ int run_steps(tild_ctx* c, int n) {
       const void* p0 = c->pos[0];
       const int cur = c->cur;
       const std::vector<char> on = tild_buckets_on(c);
+      const bool ahead = c->rho_ahead;  // whether the period's first step spreads
       cudaGraphExec_t exec = nullptr;
+      bool ahead_end = false;
       for (auto& ge : c->graphs)
-        if (ge.p0 == p0 && ge.cur == cur && ge.buckets_on == on) exec = ge.exec;
+        if (ge.p0 == p0 && ge.cur == cur && ge.buckets_on == on && ge.ahead == ahead) {
+          exec = ge.exec;
+          ahead_end = ge.ahead_end;
+        }
       if (!exec) {
         const long long l0 = c->launches;
         const int64_t step_before = c->sys[0].step;
@@ -716,11 +726,13 @@ int run_steps(tild_ctx* c, int n) {
           cudaGraphExecDestroy(c->graphs.front().exec);
           c->graphs.erase(c->graphs.begin());
         }
-        c->graphs.push_back({exec, p0, cur, on});
+        ahead_end = c->rho_ahead;
+        c->graphs.push_back({exec, p0, cur, on, ahead, ahead_end});
         c->graph_launches_per_step = per_step;
         // after capture the buffer configuration is back at (p0, cur): same as a replay
       }
       if (tild_check(c, cudaGraphLaunch(exec, c->stream), "graph launch")) return TILD_ERR_CUDA;
+      c->rho_ahead = ahead_end;
       account_replayed_steps(c, len, c->graph_launches_per_step);
       c->steps_since_sort = c->sort_interval;
       n -= len;
@@ -850,6 +862,7 @@ int sys_load(tild_ctx* c, int s, const tild_config* cfg) {
   if (nfft != (int)h.fft_cfg.size() || nfield != nfield_slot)
     return set_err(c, TILD_ERR_UNSUPPORTED, "the slot's number of FFT pair styles and of fieldphases must match");
   cudaSetDevice(c->device);
+  if (tild_drop_ahead(c)) return TILD_ERR_CUDA;
   if (tild_check(c, cudaStreamSynchronize(c->stream), "sync before load")) return TILD_ERR_CUDA;
   h.cfg = *cfg;
   set_geometry(h, *cfg);
@@ -943,6 +956,7 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
   t->sort_brick = c->sort_brick;
   t->field_layout = c->field_layout;
   t->fft_pipeline = c->fft_pipeline;
+  t->spread_ahead = c->spread_ahead;
   t->ms_per_step = 0.0;
 }
 
@@ -951,7 +965,8 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
       t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
       t->gather_mode < TILD_GATHER_DIRECT || t->gather_mode > TILD_GATHER_BOX || t->gather_cap < 1024 ||
       t->gather_cap > 3072 || t->field_layout < TILD_FIELD_LINEAR || t->field_layout > TILD_FIELD_BRICK ||
-      (t->field_layout == TILD_FIELD_BRICK && c->D != 3) || t->fft_pipeline < 0 || t->fft_pipeline > 2)
+      (t->field_layout == TILD_FIELD_BRICK && c->D != 3) || t->fft_pipeline < 0 || t->fft_pipeline > 2 ||
+      t->spread_ahead < 0 || t->spread_ahead > 1)
     return set_err(c, TILD_ERR_BAD_INPUT, "tune values out of range");
   if (t->sort_interval > 0 && !c->sort_temp) return set_err(c, TILD_ERR_UNSUPPORTED, "the context was created without sorting");
   {
@@ -967,6 +982,7 @@ int set_tune(tild_ctx* c, const tild_tune* t) {
   c->gather_cap = t->gather_cap;
   c->field_layout = t->field_layout;
   c->fft_pipeline = t->fft_pipeline;
+  c->spread_ahead = t->spread_ahead;
   if (t->sort_brick != c->sort_brick) {
     c->sort_brick = t->sort_brick;
     c->steps_since_sort = c->sort_interval;  // re-sort with the new keys at the next step
@@ -1059,6 +1075,11 @@ int engine_autotune(tild_ctx* c, int trial_steps, tild_tune* best) {
         t.gather_cap = cap;
         if (cap != cur.gather_cap) consider(t);
       }
+  }
+  for (int sa : {0, 1}) {
+    tild_tune t = cur;
+    t.spread_ahead = sa;
+    if (sa != cur.spread_ahead) consider(t);
   }
   if (c->sort_temp)
     for (int brick : tild_brick_candidates(c->D)) {
@@ -1186,6 +1207,15 @@ int snapshot_wait(tild_ctx* c, int64_t ticket) {
 }  // namespace
 
 struct tild_batch : public tild_ctx {};
+
+// The previous step's gather spread positions that the host is about to replace (or whose types,
+// charges or box change): clear the accumulator so that the next step spreads afresh.
+int tild_drop_ahead(tild_ctx* c) {
+  if (!c->rho_ahead) return TILD_OK;
+  c->rho_ahead = false;
+  return tild_check(c, cudaMemsetAsync(c->rho_fx, 0, sizeof(unsigned long long) * c->grid_total, c->stream),
+                    "clear density accumulator");
+}
 
 int tild_upload_sys(tild_ctx* c) {
   for (int s = 0; s < c->nsys; s++) c->h_sys[s].active = c->sys[s].active ? 1 : 0;

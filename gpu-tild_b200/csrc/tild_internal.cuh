@@ -131,6 +131,8 @@ struct tild_ctx {
   int sort_brick = 0;                    // brick shape and order of the sort keys (tild_sort.cu)
   int field_layout = TILD_FIELD_LINEAR;  // node order of the float4 force field g4
   int fft_pipeline = 0;                  // per shape on its stream: 1 the grid stages, 2 the whole step
+  int spread_ahead = 1;                  // integrating gathers spread x_{n+1} for the next step (order <= 1 default)
+  bool rho_ahead = false;                // rho_fx already holds the densities of the current positions
   long long g4_total = 0;
   int D = 3, P = 1;
   int nsys = 1;
@@ -213,6 +215,7 @@ struct tild_ctx {
     const void* p0;
     int cur;
     std::vector<char> buckets_on;        // grid shapes whose transforms the graph runs
+    bool ahead, ahead_end;               // rho_ahead before and after the period
   };
   std::vector<GraphEntry> graphs;
   bool use_graphs = true;
@@ -404,6 +407,7 @@ int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);
 int tild_assign_lanes(tild_ctx* c, int lanes);
+int tild_drop_ahead(tild_ctx* c);                     // positions changed on the host: clear rho_fx
 
 // Grid shapes with at least one active system: integrating steps skip the transforms of the others
 // (their systems neither move nor are gathered).  Force-only evaluations transform every shape.
@@ -416,6 +420,14 @@ inline std::vector<char> tild_buckets_on(const tild_ctx* c) {
         break;
       }
   return on;
+}
+
+// Whether this force evaluation's gather also spreads the updated positions into rho_fx for the
+// next step (integrating steps with the direct gather; the box gather keeps its shared memory
+// for the field).
+inline bool tild_spreads_ahead(const tild_ctx* c, bool integrate) {
+  return integrate && c->spread_ahead &&
+         !(c->P >= 2 && c->gather_mode == TILD_GATHER_BOX && c->field_layout == TILD_FIELD_LINEAR);
 }
 
 // Brick shapes of the spatial sort the tuner chooses from (log2 edges x | y<<4 | z<<8, bit 12 =

@@ -118,42 +118,33 @@ __device__ __forceinline__ void spread_global_kbits(const float (&W)[3][P + 1], 
 // 2^32 per unit.  Integer sums do not depend on the order of the additions, so the densities are
 // bitwise reproducible whatever the slot order or scheduling.  A chunk whose box does not fit
 // adds each node to the global accumulator directly.
-template <int D, int P>
-__global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__ pos, const float* __restrict__ charge,
-                                                     const int* __restrict__ cta_sys,
-                                                     const SysDev* __restrict__ sysd,
-                                                     unsigned long long* __restrict__ rho_fx_all, int cap,
-                                                     int* status, int blk_off) {
+//
+// The spread of one CTA's beads, positions already in registers (ok: this thread's bead is valid
+// and finite; t its type; q its charge, 0 without).  Thread 0's bead is the box origin.  Every
+// thread of the block must call it.  The spread kernel and the spreading gather share it.
+template <int D, int P, bool CH>
+__device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], int t, float q, const SysDev& sd,
+                                               unsigned long long* __restrict__ rho_fx, int cap, int* status) {
   extern __shared__ int smi[];
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ long long s_row[kMaxRows];
-  const int blk = blockIdx.x + blk_off;
-  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
   const Geom g = sd.g;
   const int T = sd.T, C = sd.C, kbits = sd.kbits;
-  unsigned long long* rho_fx = rho_fx_all + sd.grid0;
-  const int i0 = blk * blockDim.x;
-  const int i = i0 + threadIdx.x;
-  chunk_origin<D, P>(pos, i0, g, s_g0, s_min, s_max);
+  if (threadIdx.x == 0) {
+    float Wd[P + 1];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      s_g0[d] = (ok && d < D) ? axis_base<P>(xs[d], g.dx[d], Wd) : 0;
+      s_min[d] = INT_MAX;
+      s_max[d] = INT_MIN;
+    }
+  }
+  __syncthreads();
   float W[3][P + 1];
   int rel[3] = {0, 0, 0};
-  int t = 0;
-  float q = 0.f;
-  bool ok = false;
-  {
-    const float4 p = pos[i];
-    const float xs[3] = {p.x, p.y, p.z};
-    t = tild_type_of(p.w);
-    if (t != kPadType) {
-      ok = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
-      if (!ok) {
-        atomicOr(status, ST_NONFINITE_POS);
-      } else {
-        q = C ? charge[i] : 0.f;
+  if (ok) {
 #pragma unroll
-        for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
-      }
-    }
+    for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
   }
   int mn[3], ext[3];
   long long vol;
@@ -161,7 +152,7 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   const int nch = T + C;
   const long long M = g.M;
   const float ig = 1.0f / g.gvol;
-  const bool qc = C && q != 0.f;
+  const bool qc = CH && C && q != 0.f;
   if (vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
     const int tot = (int)vol * nch;
     for (int k = threadIdx.x; k < tot; k += blockDim.x) smi[k] = 0;
@@ -237,29 +228,15 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
   }
 }
 
-// Every node straight into the 64-bit global accumulator.  For order <= 1 (8-node stencils) a
-// shared box would cost more to zero, synchronise and flush than its shared atomics save, and the
-// contributions keep 2^32 per unit; for higher orders it is the tuner's alternative to the box
-// and rounds contributions exactly as the box does.
-template <int D, int P>
-__global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict__ pos, const float* __restrict__ charge,
-                                                      const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd,
-                                                      unsigned long long* __restrict__ rho_fx_all, int* status,
-                                                      int blk_off) {
-  const int blk = blockIdx.x + blk_off;
-  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
-  const int i = blk * blockDim.x + threadIdx.x;
-  const float4 p = pos[i];
-  const int t = tild_type_of(p.w);
-  if (t == kPadType) return;
-  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
-    atomicOr(status, ST_NONFINITE_POS);
-    return;
-  }
+// One valid, finite bead straight into the 64-bit global accumulator.  For order <= 1 (8-node
+// stencils) the contributions keep 2^32 per unit; for higher orders they are rounded exactly as
+// the box rounds them.
+template <int D, int P, bool CH>
+__device__ __forceinline__ void bead_spread_direct(const float (&xs)[3], int t, float q, const SysDev& sd,
+                                                   unsigned long long* __restrict__ rho_fx_all) {
   const Geom& g = sd.g;
   const int T = sd.T;
   const long long M = g.M;
-  const float xs[3] = {p.x, p.y, p.z};
   float W[3][P + 1];
   int idx[3][P + 1];
 #pragma unroll
@@ -268,11 +245,10 @@ __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict_
 #pragma unroll
     for (int a = 0; a <= P; a++) idx[d][a] = pmod(b + a, g.nx[d]);
   }
-  const float q = sd.C ? charge[i] : 0.f;
   unsigned long long* rt = rho_fx_all + sd.grid0 + (long long)t * M;
   unsigned long long* rc = rho_fx_all + sd.grid0 + (long long)T * M;
-  if (P >= 2) {  // same contributions as the shared-box kernel: results independent of the choice
-    spread_global_kbits<D, P>(W, idx, g, rt, q != 0.f ? rc : nullptr, q, 1.0f / g.gvol, sd.kbits);
+  if (P >= 2) {  // same contributions as the shared-box path: results independent of the choice
+    spread_global_kbits<D, P>(W, idx, g, rt, (CH && q != 0.f) ? rc : nullptr, q, 1.0f / g.gvol, sd.kbits);
     return;
   }
   const double sc64 = 4294967296.0 / (double)g.gvol;
@@ -287,9 +263,59 @@ __global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict_
         const long long m = D == 3 ? row + (long long)idx[2][iz] * g.nx[1] * g.nx[0] : row;
         const double W3 = (double)(D == 3 ? wxy * W[2][iz] : wxy) * sc64;
         atomicAdd(rt + m, (unsigned long long)__double2ll_rn(W3));
-        if (q != 0.f) atomicAdd(rc + m, (unsigned long long)__double2ll_rn(W3 * q));
+        if (CH && q != 0.f) atomicAdd(rc + m, (unsigned long long)__double2ll_rn(W3 * q));
       }
     }
+}
+
+// a slot's bead for the spread: valid (not padding) and finite; a non-finite one is reported
+template <int D, bool CH>
+__device__ __forceinline__ bool spread_input(const float4& p, const SysDev& sd, const float* __restrict__ charge,
+                                             int i, float (&xs)[3], int& t, float& q, int* status) {
+  xs[0] = p.x;
+  xs[1] = p.y;
+  xs[2] = p.z;
+  t = tild_type_of(p.w);
+  q = 0.f;
+  if (t == kPadType) return false;
+  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+    atomicOr(status, ST_NONFINITE_POS);
+    return false;
+  }
+  if (CH && sd.C) q = charge[i];
+  return true;
+}
+
+template <int D, int P, bool CH>
+__global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__ pos, const float* __restrict__ charge,
+                                                     const int* __restrict__ cta_sys,
+                                                     const SysDev* __restrict__ sysd,
+                                                     unsigned long long* __restrict__ rho_fx_all, int cap,
+                                                     int* status, int blk_off) {
+  const int blk = blockIdx.x + blk_off;
+  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
+  const int i = blk * blockDim.x + threadIdx.x;
+  float xs[3], q;
+  int t;
+  const bool ok = spread_input<D, CH>(pos[i], sd, charge, i, xs, t, q, status);
+  cta_spread_box<D, P, CH>(ok, xs, t, q, sd, rho_fx_all + sd.grid0, cap, status);
+}
+
+// Every node straight into the 64-bit global accumulator: always for order <= 1, where a shared
+// box would cost more to zero, synchronise and flush than its shared atomics save; for higher
+// orders it is the tuner's alternative to the box.
+template <int D, int P, bool CH>
+__global__ void __launch_bounds__(256) k_spread_direct(const float4* __restrict__ pos, const float* __restrict__ charge,
+                                                      const int* __restrict__ cta_sys, const SysDev* __restrict__ sysd,
+                                                      unsigned long long* __restrict__ rho_fx_all, int* status,
+                                                      int blk_off) {
+  const int blk = blockIdx.x + blk_off;
+  const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
+  const int i = blk * blockDim.x + threadIdx.x;
+  float xs[3], q;
+  int t;
+  if (spread_input<D, CH>(pos[i], sd, charge, i, xs, t, q, status))
+    bead_spread_direct<D, P, CH>(xs, t, q, sd, rho_fx_all);
 }
 
 // fixed-point grid -> FP32 density over every system's channels, clearing the accumulator for the
@@ -580,67 +606,83 @@ __device__ __forceinline__ void bead_epilogue(int i, const float4& p, int t, flo
   }
 }
 
-template <int D, int P, bool INTEG, bool XW>
+// SPR (integrating launches only): after the update the kernel spreads x_{n+1} into the density
+// accumulator for the next step, through the shared box (1) or the global atomics (2), so the
+// next step needs no spread kernel.  Inactive systems spread their held positions.  The integer
+// sums are those of the spread kernel, bitwise.
+template <int D, int P, bool INTEG, bool XW, bool CH, int SPR>
 __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 : 4)))) k_gather(
     const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
     const float* __restrict__ charge, const float4* __restrict__ g4_all, const int* __restrict__ cta_sys,
     const SysDev* __restrict__ sysd, float* __restrict__ f_out, int f_sys, curandStateXORWOW_t* __restrict__ xw,
-    int layout, int* status, int blk_off) {
+    int layout, unsigned long long* __restrict__ rho_fx_all, int spread_cap, int* status, int blk_off) {
+  static_assert(SPR == 0 || INTEG, "only integrating launches spread ahead");
   const int s = cta_sys[blockIdx.x + blk_off];
   const SysDev& sd = sysd[s];
   const int i = (blockIdx.x + blk_off) * blockDim.x + threadIdx.x;
-  if (!sd.active) {
-    if (INTEG) pos_io[i] = pos_in[i];  // inactive systems keep x_n through the buffer rotation
-    return;
-  }
   const float4 p = pos_in[i];
   const int t = tild_type_of(p.w);
-  if (t == kPadType) return;
   float x[3] = {p.x, p.y, p.z};
-  if (!(isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z)))) {
+  const bool finite = isfinite(p.x) && isfinite(p.y) && (D == 2 || isfinite(p.z));
+  const int C = sd.C;
+  const float q = (CH && C && t != kPadType) ? charge[i] : 0.f;
+  bool sp = false;  // x (after the update) is spread ahead
+  if (!sd.active) {  // one system per CTA: every thread takes this branch together
+    if (INTEG) pos_io[i] = p;  // inactive systems keep x_n through the buffer rotation
+    if (SPR == 0) return;
+    sp = t != kPadType && finite;  // held positions are spread too
+    if (t != kPadType && !finite) atomicOr(status, ST_NONFINITE_POS);
+  } else if (t != kPadType && !finite) {
     atomicOr(status, ST_NONFINITE_POS);
-    return;  // left in place; the host reports TILD_ERR_NAN
-  }
-  const Geom& g = sd.g;
-  const long long Mb = sd.Mb;
-  const int T = sd.T, C = sd.C;
-  const float4* g4 = g4_all + sd.g4_0;
-  // loads that do not depend on the stencil are issued before it, so their latency overlaps
-  const int info = bond_info[i];
-  const int nb = info & 3;
-  float4 pj[3];
+    if (SPR == 0) return;  // left in place; the host reports TILD_ERR_NAN
+  } else if (t != kPadType) {
+    const Geom& g = sd.g;
+    const long long Mb = sd.Mb;
+    const int T = sd.T;
+    const float4* g4 = g4_all + sd.g4_0;
+    // loads that do not depend on the stencil are issued before it, so their latency overlaps
+    const int info = bond_info[i];
+    const int nb = info & 3;
+    float4 pj[3];
 #pragma unroll
-  for (int bb = 0; bb < 3; bb++)
-    if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
-  const int bid = bead_id[i];
-  float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
+    for (int bb = 0; bb < 3; bb++)
+      if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
+    const int bid = bead_id[i];
+    float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (INTEG) po = pos_io[i];  // x_{n-1} (GJF xo)
 
-  float f[3] = {0.f, 0.f, 0.f};
-  {
-    float W[3][P + 1];
-    int idx[3][P + 1];
+    float f[3] = {0.f, 0.f, 0.f};
+    {
+      float W[3][P + 1];
+      int idx[3][P + 1];
 #pragma unroll
-    for (int d = 0; d < D; d++) {
-      const int b = axis_base<P>(x[d], g.dx[d], W[d]);
+      for (int d = 0; d < D; d++) {
+        const int b = axis_base<P>(x[d], g.dx[d], W[d]);
 #pragma unroll
-      for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
-    }
-    int o[3][P + 1];
-    field_offsets<D, P>(idx, layout, g, o);
-    if (C) {
-      const float q = charge[i];
-      if (q != 0.f) {
+        for (int a = 0; a <= P; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
+      }
+      int o[3][P + 1];
+      field_offsets<D, P>(idx, layout, g, o);
+      if (CH && C && q != 0.f) {
         float e[3] = {0.f, 0.f, 0.f};
         gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
 #pragma unroll
         for (int d = 0; d < D; d++) f[d] += e[d] * q;
       }
+      gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
     }
-    gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
+    bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
+    if (SPR != 0) {
+      sp = isfinite(x[0]) && isfinite(x[1]) && (D == 2 || isfinite(x[2]));
+      if (!sp) atomicOr(status, ST_NONFINITE_POS);
+    }
+  } else if (SPR == 0) {
+    return;  // padding slot
   }
-  bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
+  if constexpr (SPR == 1) cta_spread_box<D, P, CH>(sp, x, t, q, sd, rho_fx_all + sd.grid0, spread_cap, status);
+  if constexpr (SPR == 2)
+    if (sp) bead_spread_direct<D, P, CH>(x, t, q, sd, rho_fx_all);
 }
 
 // The same stencil sums read from a shared-memory box: the CTA's 256 slots (spatially sorted, so
@@ -674,7 +716,7 @@ __device__ __forceinline__ void box_gather4(const float4* __restrict__ B, const 
     }
 }
 
-template <int D, int P, bool INTEG, bool XW>
+template <int D, int P, bool INTEG, bool XW, bool CH>
 __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
     const float4* __restrict__ pos_in, float4* __restrict__ pos_io, float* __restrict__ noise,
     const int* __restrict__ bead_id, const int* __restrict__ bond_nbr, const int* __restrict__ bond_info,
@@ -730,7 +772,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
   const long long Mb = sd.Mb;  // the box gather runs on the linear layout
   const int T = sd.T, C = sd.C, nch = T + C;
   const float4* g4 = g4_all + sd.g4_0;
-  const float q = (C && ok) ? charge[i] : 0.f;
+  const float q = (CH && C && ok) ? charge[i] : 0.f;
   float f[3] = {0.f, 0.f, 0.f};
   const int ex = ext[0], ey = ext[1], ez = ext[2];
   if (vol * nch <= box_cap && ex <= 64 && ey * ez <= kMaxRows) {
@@ -772,7 +814,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
       int lb[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < D; d++) lb[d] = rel[d] - mn[d];
-      if (C && q != 0.f) {
+      if (CH && C && q != 0.f) {
         float e[3] = {0.f, 0.f, 0.f};
         box_gather4<D, P>(sbox + (long long)T * vol, W, lb, ex, ex * ey, e);
 #pragma unroll
@@ -788,7 +830,7 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
       for (int a = 0; a <= P; a++) idx[d][a] = pmod(base[d] + a, g.nx[d]);
     int o[3][P + 1];
     field_offsets<D, P>(idx, TILD_FIELD_LINEAR, g, o);
-    if (C && q != 0.f) {
+    if (CH && C && q != 0.f) {
       float e[3] = {0.f, 0.f, 0.f};
       gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
 #pragma unroll
@@ -820,55 +862,92 @@ struct BeadRange {
 };
 inline BeadRange all_beads(tild_ctx* c) { return {c->stream, 0, c->n_cta_bead}; }
 
-template <int D, int P>
-void launch_spread(tild_ctx* c, BeadRange r) {
-  if (r.n == 0) return;
+// CH: some system of the engine has charges (the kernels without it carry no charge code)
+template <int D, int P, bool CH>
+void launch_spread_k(tild_ctx* c, BeadRange r) {
   if (P <= 1 || c->spread_mode == TILD_SPREAD_DIRECT) {
-    k_spread_direct<D, P><<<r.n, kTile, 0, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
-                                                    c->d_status, r.off);
+    k_spread_direct<D, P, CH><<<r.n, kTile, 0, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
+                                                        c->d_status, r.off);
   } else if constexpr (P >= 2) {
     static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
     const unsigned long long bit = 1ull << (c->device & 63);
     if (!(attr_devices.load() & bit)) {
-      cudaFuncSetAttribute(k_spread_tiled<D, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_spread_tiled<D, P, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(int) * 12288));
       attr_devices.fetch_or(bit);
     }
     const size_t smem = sizeof(int) * (size_t)c->spread_cap;
-    k_spread_tiled<D, P><<<r.n, kTile, smem, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
-                                                      c->spread_cap, c->d_status, r.off);
+    k_spread_tiled<D, P, CH><<<r.n, kTile, smem, r.st>>>(c->pos[c->cur], c->charge, c->cta_bead, c->d_sys, c->rho_fx,
+                                                          c->spread_cap, c->d_status, r.off);
   }
 }
 
-template <int D, int P, bool I, bool X>
-void launch_gather_k(tild_ctx* c, float* f_out, int f_sys, BeadRange r) {
+template <int D, int P>
+void launch_spread(tild_ctx* c, BeadRange r) {
   if (r.n == 0) return;
+  if (c->any_charges) launch_spread_k<D, P, true>(c, r);
+  else launch_spread_k<D, P, false>(c, r);
+}
+
+template <int D, int P, bool I, bool X, bool CH>
+void launch_gather_k(tild_ctx* c, float* f_out, int f_sys, BeadRange r) {
   if (P >= 2 && c->gather_mode == TILD_GATHER_BOX && c->field_layout == TILD_FIELD_LINEAR) {
     static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
     const unsigned long long bit = 1ull << (c->device & 63);
     if (!(attr_devices.load() & bit)) {
-      cudaFuncSetAttribute(k_gather_box<D, P, I, X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_gather_box<D, P, I, X, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(float4) * kGatherBoxMax));
       attr_devices.fetch_or(bit);
     }
-    k_gather_box<D, P, I, X><<<r.n, kTile, sizeof(float4) * (size_t)c->gather_cap, r.st>>>(
+    k_gather_box<D, P, I, X, CH><<<r.n, kTile, sizeof(float4) * (size_t)c->gather_cap, r.st>>>(
         c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
         c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->gather_cap, c->d_status, r.off);
     return;
   }
-  k_gather<D, P, I, X><<<r.n, kTile, 0, r.st>>>(
+  if constexpr (I) {
+    if (tild_spreads_ahead(c, true)) {
+      if constexpr (P >= 2) {
+        if (c->spread_mode == TILD_SPREAD_TILED) {  // spread ahead through the shared box
+          static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
+          const unsigned long long bit = 1ull << (c->device & 63);
+          if (!(attr_devices.load() & bit)) {
+            cudaFuncSetAttribute(k_gather<D, P, I, X, CH, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(int) * 12288));
+            attr_devices.fetch_or(bit);
+          }
+          k_gather<D, P, I, X, CH, 1><<<r.n, kTile, sizeof(int) * (size_t)c->spread_cap, r.st>>>(
+              c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
+              c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->rho_fx, c->spread_cap,
+              c->d_status, r.off);
+          return;
+        }
+      }
+      k_gather<D, P, I, X, CH, 2><<<r.n, kTile, 0, r.st>>>(  // spread ahead by global atomics
+          c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
+          c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->rho_fx, 0, c->d_status, r.off);
+      return;
+    }
+  }
+  k_gather<D, P, I, X, CH, 0><<<r.n, kTile, 0, r.st>>>(
       c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
-      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->d_status, r.off);
+      c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, nullptr, 0, c->d_status, r.off);
+}
+
+template <int D, int P, bool I, bool X>
+void launch_gather_ch(tild_ctx* c, float* f_out, int f_sys, BeadRange r) {
+  if (r.n == 0) return;
+  if (c->any_charges) launch_gather_k<D, P, I, X, true>(c, f_out, f_sys, r);
+  else launch_gather_k<D, P, I, X, false>(c, f_out, f_sys, r);
 }
 
 template <int D, int P>
 void launch_gather(tild_ctx* c, bool integ, float* f_out, int f_sys, BeadRange r) {
   const bool xw = c->rng == TILD_RNG_XORWOW;
   if (integ) {
-    if (xw) launch_gather_k<D, P, true, true>(c, f_out, f_sys, r);
-    else launch_gather_k<D, P, true, false>(c, f_out, f_sys, r);
+    if (xw) launch_gather_ch<D, P, true, true>(c, f_out, f_sys, r);
+    else launch_gather_ch<D, P, true, false>(c, f_out, f_sys, r);
   } else {
-    launch_gather_k<D, P, false, false>(c, f_out, f_sys, r);
+    launch_gather_ch<D, P, false, false>(c, f_out, f_sys, r);
   }
 }
 
@@ -959,11 +1038,14 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       const Bucket& b = c->buckets[bi];
       cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
       const BeadRange r{bs, b.cta_bead0, b.n_cta_bead};
-      if (c->D == 3) dispatch_p_spread<3>(c, r);
-      else dispatch_p_spread<2>(c, r);
+      if (!c->rho_ahead) {
+        if (c->D == 3) dispatch_p_spread<3>(c, r);
+        else dispatch_p_spread<2>(c, r);
+        c->launches++;
+      }
       const long long n = (long long)b.channels * b.nx[0] * b.nx[1] * b.nx[2];
       k_fix_to_float<<<nblk(n, 256), 256, 0, bs>>>(c->rho_fx + b.grid0, c->rho + b.grid0, n);
-      c->launches += 2;
+      c->launches++;
       if (on[bi]) {
         if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
         if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
@@ -979,12 +1061,16 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
     }
     if (join(c)) return TILD_ERR_CUDA;
     if (tild_check(c, cudaGetLastError(), "shape pipeline")) return TILD_ERR_CUDA;
+    c->rho_ahead = false;  // the conversions cleared the accumulator
     return tild_finish_forces(c, integrate, f_bead, f_sys, true, true);
   }
   tild_mark(c, STAGE_SPREAD);
-  if (c->D == 3) dispatch_p_spread<3>(c, all_beads(c));
-  else dispatch_p_spread<2>(c, all_beads(c));
-  c->launches++;
+  if (!c->rho_ahead) {  // else the previous step's gather spread these positions already
+    if (c->D == 3) dispatch_p_spread<3>(c, all_beads(c));
+    else dispatch_p_spread<2>(c, all_beads(c));
+    c->launches++;
+  }
+  c->rho_ahead = false;  // the conversion below clears the accumulator
   if (c->fft_pipeline >= 1 && c->lanes > 0) {
     // each grid shape runs conversion, R2C, k-space multiply and C2R in order on its stream, so
     // one shape's transforms overlap another's element-wise passes (one profiling stage)
@@ -1062,6 +1148,7 @@ int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bo
     c->launches++;
     if (tild_check(c, cudaGetLastError(), "gather")) return TILD_ERR_CUDA;
   }
+  c->rho_ahead = tild_spreads_ahead(c, integrate);
   if (integrate) {
     tild_mark(c, STAGE_TAIL);
     k_advance_steps<<<nblk(c->nsys, 128), 128, 0, c->stream>>>(c->d_sys, c->nsys);

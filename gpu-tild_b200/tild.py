@@ -64,7 +64,7 @@ class Tune(C.Structure):
     _fields_ = [("spread_mode", C.c_int32), ("spread_cap", C.c_int32), ("sort_interval", C.c_int32),
                 ("fft_streams", C.c_int32), ("gather_mode", C.c_int32), ("gather_cap", C.c_int32),
                 ("sort_brick", C.c_int32), ("field_layout", C.c_int32), ("fft_pipeline", C.c_int32),
-                ("ms_per_step", C.c_double)]
+                ("spread_ahead", C.c_int32), ("ms_per_step", C.c_double)]
 
     def as_dict(self) -> dict:
         return {"spread_mode": "tiled" if self.spread_mode == SPREAD_TILED else "direct",
@@ -72,6 +72,7 @@ class Tune(C.Structure):
                 "fft_streams": self.fft_streams, "gather_mode": ("direct", "box")[self.gather_mode],
                 "gather_cap_nodes": self.gather_cap, "sort_brick": hex(self.sort_brick),
                 "field_layout": ("linear", "brick")[self.field_layout], "fft_pipeline": int(self.fft_pipeline),
+                "spread_ahead": int(self.spread_ahead),
                 "ms_per_step": self.ms_per_step}
 
 

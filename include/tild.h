@@ -296,6 +296,9 @@ typedef struct tild_tune {
                              1 runs each shape's fixed-point conversion, R2C, k-space multiply, C2R
                              and interleave in sequence on its own stream; 2 runs each shape's whole
                              step (spread to gather) on its stream (without fieldphase styles) */
+  int32_t spread_ahead;   /* 1: an integrating step's gather (DIRECT) also spreads the updated positions
+                             for the next step, which then runs no spread kernel; 0: a spread kernel
+                             at the start of every step */
   double ms_per_step;     /* tild_autotune: measured step time with these settings */
 } tild_tune;
 int32_t tild_get_tune(tild_ctx* ctx, tild_tune* out);

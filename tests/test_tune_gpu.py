@@ -36,6 +36,9 @@ def run(s, tune=None, steps=70):
     {"gather_mode": tild.GATHER_BOX, "gather_cap": 1024},   # most chunks fall back to global reads
     {"field_layout": tild.FIELD_BRICK},
     {"field_layout": tild.FIELD_BRICK, "gather_mode": tild.GATHER_BOX},   # box needs linear: direct runs
+    {"spread_ahead": 1},                  # the gather spreads for the next step (shared box)
+    {"spread_ahead": 1, "spread_mode": tild.SPREAD_DIRECT},
+    {"spread_ahead": 1, "spread_cap": 1024},
 ])
 def test_every_setting_gives_the_same_trajectory(tune):
     s = p3_system()
@@ -110,3 +113,31 @@ def test_shape_pipeline_gives_the_same_trajectories(level):
             out.append([B.get_state(i)[0] for i in range(3)])
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("pmeorder", [1, 3])
+def test_spread_ahead_after_host_changes(pmeorder):
+    """The gather spreads x_{n+1} for the next step; positions replaced on the host must discard
+    those densities, and a force-only evaluation may use them."""
+    s = small_diblock(3, pmeorder, nx=(20, 18, 16), box=(10.0, 9.0, 8.0), n_chains=150, N=10, seed=33)
+    ref = run(s, {"spread_ahead": 0}, steps=40)
+    with tild.Context(s) as c:
+        t = c.get_tune()
+        t.spread_ahead = 1
+        c.set_tune(t)
+        c.step(40)
+        mid = c.get_state()
+        f_mid = c.forces()                       # force-only evaluation on the spread-ahead densities
+        c.step(5)
+        c.set_state(s.x)                         # back to the start: the pending densities are stale
+        c.set_step(0)
+        c.step(40)
+        again = c.get_state()
+    with tild.Context(s) as c:
+        c.set_state(mid[0], mid[1], mid[2])
+        c.set_step(40)
+        f_fresh = c.forces()
+    assert np.array_equal(f_mid, f_fresh)
+    for a, b, r in zip(mid, again, ref):
+        assert np.array_equal(a, b)
+        assert np.array_equal(a, r)
