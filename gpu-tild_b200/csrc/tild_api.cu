@@ -124,6 +124,11 @@ int validate(const tild_config* cfg, std::string& why) {
     if (cfg->nx[d] < 1 || !(cfg->box[d] > 0.f)) { why = "grid sizes and box lengths must be positive"; return TILD_ERR_BAD_INPUT; }
     if (cfg->nx[d] < cfg->pmeorder + 1) { why = "grid smaller than the assignment stencil"; return TILD_ERR_BAD_INPUT; }
   }
+  {
+    long long m = 1;
+    for (int d = 0; d < cfg->dim; d++) m *= cfg->nx[d];
+    if (m >= (1ll << 31)) { why = "grids of 2^31 points or more are not supported"; return TILD_ERR_BAD_INPUT; }
+  }
   if (cfg->n_styles < 0 || cfg->n_styles > TILD_MAX_STYLES) { why = "too many pair styles"; return TILD_ERR_BAD_INPUT; }
   for (int i = 0; i < cfg->n_styles; i++) {
     const tild_pair_style& s = cfg->styles[i];

@@ -25,16 +25,20 @@ constexpr double kInvFix = 1.0 / 4294967296.0;  // the global accumulator holds 
 constexpr int kMaxRows = 1024;                  // (y, z) rows of a shared-memory spread box
 constexpr int kGatherBoxMax = 3072;             // float4 nodes of the gather's shared box (48 KB)
 
-__device__ __forceinline__ int fold_rel(int r, int N) {
-  r %= N;
-  if (r < 0) r += N;
-  if (r > N / 2) r -= N;
-  return r;
-}
-
+// n mod N in [0, N); indices within one period of the grid (nearly all) take no division
 __device__ __forceinline__ int pmod(int n, int N) {
+  if ((unsigned)n < (unsigned)N) return n;
+  if (n < 0 && n >= -N) return n + N;
+  if (n >= N && n - N < N) return n - N;
   n %= N;
   return n < 0 ? n + N : n;
+}
+
+// r folded into (-N/2, N/2]
+__device__ __forceinline__ int fold_rel(int r, int N) {
+  r = pmod(r, N);
+  if (r > N / 2) r -= N;
+  return r;
 }
 
 // Chunk bounding box of the beads' stencil bases, relative to the chunk's first bead.
@@ -363,10 +367,11 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   const float* utab = utab_all + sd.utab0 + h;
   const float2* rhok = rhok_all + sd.spec0;
   const float* kd = kd_all + sd.kd0;
-  const int ix = (int)(h % g.nxh);
-  const long long r = h / g.nxh;
-  const int iy = (int)(r % g.nx[1]);
-  const int iz = (int)(r / g.nx[1]);
+  // 32-bit index arithmetic: grids hold fewer than 2^31 points (tild_create checks)
+  const unsigned hu = (unsigned)h, rr = hu / (unsigned)g.nxh;
+  const int ix = (int)(hu - rr * (unsigned)g.nxh);
+  const int iy = (int)(rr % (unsigned)g.nx[1]);
+  const int iz = (int)(rr / (unsigned)g.nx[1]);
   float kv[3];
   kv[0] = kd[ix];
   kv[1] = kd[g.nx[0] + iy];
@@ -456,10 +461,10 @@ __global__ void k_interleave(const float* __restrict__ planar_all, float4* __res
   const long long m = (long long)(blk - blk0[s]) * blockDim.x + threadIdx.x;
   if (m >= M) return;
   long long dst = m;
-  if (layout != TILD_FIELD_LINEAR) {
-    const int x = (int)(m % g.nx[0]);
-    const long long r = m / g.nx[0];
-    const int y = (int)(r % g.nx[1]), z = (int)(r / g.nx[1]);
+  if (layout != TILD_FIELD_LINEAR) {  // 32-bit index arithmetic: grids hold fewer than 2^31 points
+    const unsigned mu = (unsigned)m, r = mu / (unsigned)g.nx[0];
+    const int x = (int)(mu - r * (unsigned)g.nx[0]);
+    const int y = (int)(r % (unsigned)g.nx[1]), z = (int)(r / (unsigned)g.nx[1]);
     dst = tild_field_off(layout, 0, x, g) + tild_field_off(layout, 1, y, g) + tild_field_off(layout, 2, z, g);
   }
   const float* planar = planar_all + sd.grid0 * D;
