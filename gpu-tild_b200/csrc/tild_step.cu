@@ -298,7 +298,10 @@ __global__ void __launch_bounds__(256) k_spread_tiled(const float4* __restrict__
                                                      int* status, int blk_off) {
   const int blk = blockIdx.x + blk_off;
   const SysDev& sd = sysd[cta_sys[blk]];  // inactive systems too (see k_fix_to_float)
-  const int i = blk * blockDim.x + threadIdx.x;
+  static_assert(kTile == 256, "the lane-to-slot map below assumes 8 warps of 32");
+  // lane l of warp w takes slot 8 l + w: a warp's beads lie in distinct cells, so its shared
+  // atomics meet fewer equal addresses; thread 0 keeps slot 0, the box origin
+  const int i = blk * blockDim.x + (((threadIdx.x & 31) << 3) | (threadIdx.x >> 5));
   float xs[3], q;
   int t;
   const bool ok = spread_input<D, CH>(pos[i], sd, charge, i, xs, t, q, status);
