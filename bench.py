@@ -198,6 +198,9 @@ def run_serving(args):
 def make_system(workload: str):
     if workload == "blend":
         return ts.homopolymer_blend(), "blend_2.6M_128^3_gaussian_erf_p3_GJF"
+    if workload == "blend_half":  # half the blend (same density and stencil) for multi-pass ncu captures
+        return (ts.homopolymer_blend(n_chains=65000, box=(64.0, 64.0, 32.0), nx=(128, 128, 64)),
+                "blend_1.3M_128x128x64_gaussian_erf_p3_GJF")
     if workload == "diblock":
         return ts.diblock_melt(), "diblock_40k_40^3_gaussian_p1_GJF"
     if workload == "coacervate":
@@ -470,7 +473,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="blend", choices=["blend", "diblock", "coacervate", "ensemble", "serving"])
+    ap.add_argument("--workload", default="blend", choices=["blend", "blend_half", "diblock", "coacervate", "ensemble", "serving"])
     ap.add_argument("--nsys", type=int, default=256)
     ap.add_argument("--jobs", type=int, default=300, help="serving: number of jobs in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: mean arrivals per second")
