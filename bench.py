@@ -4,12 +4,16 @@ Workload (default, --workload blend): A/B homopolymer blend, 130,000 chains x N=
 box 64^3, grid 128^3, three gaussian_erf pair styles (R_p = 0.5, smearing 0.5, kappa = 50,
 chi = 0.2), 4th-order assignment (64-point stencil), GJF, dt = 0.005, seeded synthetic chains.
 A "step" is one full TILD step: spread, R2C, k-space multiply, C2R, gather + bonds + GJF.
+Other workloads: diblock (40k beads, 40^3), coacervate (220k, 96^3, charges, EM), ensemble
+(256 systems batched), serving (Poisson job stream), blend_half (the blend at half the volume,
+for multi-pass profiler captures).
 
 Arms:
   --impl ours       (default) libtild through its C ABI.  value: device-timed (CUDA events on
                     the context stream) K steps with the state resident in HBM; e2e: the same K
-                    steps through the public API from host buffers (initial state uploaded, an
-                    observable record read back every 100 steps, final positions read back).
+                    steps through the public API from page-locked host buffers (initial state
+                    uploaded, an observable record read back every 128 steps, final positions
+                    read back).
   --impl reference  the reference algorithm on the host cores: the FP64 oracle port
                     (oracle/tild_oracle.c, OpenMP over all host threads) on a bounded sample of
                     the same workload.  When the reference's own CUDA build is present
