@@ -351,6 +351,8 @@ def run_ours(args):
     x_in = tild.HostArray((s.ns, s.dim))   # page-locked host buffers, filled/allocated before timing
     x_in.array[:] = s.x
     x_out = tild.HostArray((s.ns, s.dim))
+    ctx.observables()   # untimed: the first call allocates the reduction scratch once
+    ctx.sync()
     t0 = time.perf_counter()
     ctx.set_state(x_in.array)
     done = 0
