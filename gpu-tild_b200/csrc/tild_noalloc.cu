@@ -14,8 +14,14 @@
 //  * every call on a device uses the same array and leaves its partial sums there; each call
 //    writes every slot it later reads, so no clearing is needed, but two calls whose kernels
 //    overlap on the GPU (different streams, no ordering between them) race on the array;
-//  * the first call on each device (with that device current) looks up the array's device
-//    address; make that first call before any stream capture.
+//  * the array's device address is looked up (cudaGetSymbolAddress) on every call made outside
+//    stream capture, so a device reset or a new primary context between calls is picked up;
+//    a call made while its stream is capturing uses the address the last uncaptured call on
+//    that device and context found, so make one call outside capture first (again after any
+//    device reset);
+//  * a CUDA error already pending on the calling thread is reported and left pending: the
+//    call launches nothing and returns TILD_ERR_CUDA, and the caller's error is not consumed.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <mutex>
@@ -32,7 +38,28 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_bond_partials[TILD_NOALLOC_MAX_BLOCKS * kVals];
 
 std::mutex g_mutex;
-double* g_partials_addr[kMaxDevices] = {nullptr};
+struct CachedAddr {
+  double* addr = nullptr;
+  void* ctx = nullptr;  // the context the address belongs to
+};
+CachedAddr g_partials[kMaxDevices];
+
+// The calling thread's current context (driver entry point through the runtime, so the library
+// needs no link against the driver library); nullptr when it cannot be had.
+void* current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<Fn>(p);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 
 struct BondArgs {
   float L[3], Lh[3];
@@ -49,14 +76,16 @@ __global__ void __launch_bounds__(kThreads) k_bond_partials(const float* __restr
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < a.ns) {
     const int n = nb[i];
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+    if (n < 0 || n > TILD_MAX_BONDS) v[0] = qnan;  // corrupt topology: poison the result
     for (int b = 0; b < n && b < TILD_MAX_BONDS; b++) {
       const int j = bto[3 * i + b];
       const int bt = bty[3 * i + b];
-      if (j < i) continue;
-      if (j >= a.ns || bt < 0 || bt >= a.nbt) {  // corrupt topology: poison the result
-        v[0] = __longlong_as_double(0x7ff8000000000000LL);
+      if (j < 0 || j >= a.ns || bt < 0 || bt >= a.nbt) {  // checked before the j < i skip
+        v[0] = qnan;
         continue;
       }
+      if (j < i) continue;
       double dr[3] = {0, 0, 0}, mdr2 = 0.0;
       for (int d = 0; d < a.D; d++) {
         const float xi = x[(long long)i * a.D + d], xj = x[(long long)j * a.D + d];
@@ -132,16 +161,32 @@ extern "C" int32_t tild_bond_observables_noalloc(const float* d_x, const int32_t
             (int)ns, (int)TILD_NOALLOC_MAX_BEADS);
     return TILD_ERR_BAD_INPUT;
   }
+  // an error left by earlier work on this thread is the caller's: report it, keep it pending
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    fprintf(stderr, "tild_bond_observables_noalloc: a CUDA error from earlier work is pending (%s); nothing launched\n",
+            cudaGetErrorString(pending));
+    return TILD_ERR_CUDA;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     fprintf(stderr, "tild_bond_observables_noalloc: no usable current device\n");
     return TILD_ERR_CUDA;
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    fprintf(stderr, "tild_bond_observables_noalloc: invalid stream\n");
+    return TILD_ERR_BAD_INPUT;
+  }
+  void* ctx = current_context();
   double* partials = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mutex);
-    if (!g_partials_addr[dev]) {
+    CachedAddr& ca = g_partials[dev];
+    if (cap == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_bond_partials);
       if (e != cudaSuccess || !p) {
@@ -149,9 +194,14 @@ extern "C" int32_t tild_bond_observables_noalloc(const float* d_x, const int32_t
         fprintf(stderr, "tild_bond_observables_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
         return TILD_ERR_CUDA;
       }
-      g_partials_addr[dev] = static_cast<double*>(p);
+      ca.addr = static_cast<double*>(p);
+      ca.ctx = ctx;
+    } else if (!ca.addr || ca.ctx != ctx) {
+      fprintf(stderr, "tild_bond_observables_noalloc: called under stream capture before any call outside capture "
+                      "on this device and context\n");
+      return TILD_ERR_STATE;
     }
-    partials = g_partials_addr[dev];
+    partials = ca.addr;
   }
   BondArgs a;
   double V = 1.0;
@@ -169,7 +219,6 @@ extern "C" int32_t tild_bond_observables_noalloc(const float* d_x, const int32_t
   a.D = dim;
   const int np = (dim == 2) ? 3 : 6;
   const int nblocks = ns > 0 ? (ns + kThreads - 1) / kThreads : 1;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   k_bond_partials<<<nblocks, kThreads, 0, st>>>(d_x, d_n_bonds, d_bonded_to, d_bond_type, a, partials);
   k_bond_final<<<1, 32, 0, st>>>(partials, nblocks, 1.0 / V / (double)dim, np, d_out);
   const cudaError_t e = cudaGetLastError();

@@ -184,6 +184,11 @@ void read_config(const std::string& path, Script& s, bool with_charges) {
 }
 
 // ---- read_resume (config_utils.cu:405-454): positions by line order --------------------------
+// The header is skipped as the reference skips it.  Atom lines ("id type mol x y z [q]", the
+// trajectory format of write_lammps_traj, config_utils.cu:366-403) are read one line at a time:
+// the reference's "%f " after the last coordinate also consumes the newline, so in 3-D frames
+// without charges its fgets(tt, 5) then eats the start of the next line; reading whole lines
+// takes every frame the reference writes, 2-D, 3-D, with and without charges.
 void read_resume(const std::string& path, Script& s) {
   FILE* inp = fopen(path.c_str(), "r");
   if (!inp) die("Failed to open " + path + "!");
@@ -198,20 +203,26 @@ void read_resume(const std::string& path, Script& s) {
   for (int k = 0; k < 6; k++)
     if (!fgets(tt, 100, inp)) break;
   const int Dim = s.Dim;
+  char line[512];
   for (int i = 0; i < s.sys.ns; i++) {
-    int t1, t2, t3;
-    if (fscanf(inp, "%d %d %d  ", &t1, &t2, &t3) != 3) die("Premature end of resume file");
-    for (int j = 0; j < Dim; j++)
-      if (fscanf(inp, "%f ", &s.sys.x[(size_t)i * Dim + j]) != 1) die("Premature end of resume file");
-    for (int j = Dim; j < 3; j++) {
-      float f1;
-      if (fscanf(inp, "%f", &f1) != 1) die("Premature end of resume file");
+    if (!fgets(line, sizeof line, inp)) {
+      fclose(inp);
+      die("Premature end of resume file");
     }
-    if (s.do_charges) {
-      float f1;
-      if (fscanf(inp, "%f", &f1) != 1) die("Premature end of resume file");
+    int t1, t2, t3, used = 0;
+    const char* q = line;
+    if (sscanf(q, "%d %d %d%n", &t1, &t2, &t3, &used) != 3) {
+      fclose(inp);
+      die("Premature end of resume file");
     }
-    if (!fgets(tt, 5, inp)) tt[0] = 0;
+    q += used;
+    for (int j = 0; j < Dim; j++) {
+      if (sscanf(q, "%f%n", &s.sys.x[(size_t)i * Dim + j], &used) != 1) {
+        fclose(inp);
+        die("Premature end of resume file");
+      }
+      q += used;
+    }
   }
   fclose(inp);
   std::cout << "SUCCESSFULLY READ RESUME FILE" << std::endl;

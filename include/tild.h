@@ -341,8 +341,13 @@ void tild_host_free(void* p);
  * scratch is a fixed device array of TILD_NOALLOC_MAX_BLOCKS x 7 doubles (229 KB) that every GPU
  * loading the library keeps until exit, so ns is limited to TILD_NOALLOC_MAX_BEADS; larger ns
  * returns TILD_ERR_BAD_INPUT.  All calls share that array: calls that overlap on the GPU race.
- * The first call on each device (that device current) looks the array up; make it before any
- * stream capture.
+ * Every call made outside stream capture looks the array's device address up again (so a device
+ * reset between calls is harmless); a call on a capturing stream reuses the address the last
+ * uncaptured call on that device and context found, and returns TILD_ERR_STATE if there was
+ * none: make one call outside capture first, and again after a device reset.  A CUDA error
+ * already pending on the calling thread is left pending and reported as TILD_ERR_CUDA with
+ * nothing launched.  Corrupt topology (a bond count outside 0..3, a partner or bond type out of
+ * range) makes d_out[0] NaN.
  *   d_x[ns*dim] float, d_n_bonds[ns], d_bonded_to[ns*3], d_bond_type[ns*3]: device arrays in the
  *   read_config layout; box[3], bond_k[], bond_req[]: host arrays; d_out (device, FP64):
  *   d_out[0] = bond energy, d_out[1..nP] = bond virial / (V * dim) (nP = 6 in 3D, 3 in 2D);

@@ -8,7 +8,13 @@
 //   <out>_w.bin    d_grid_W                                 float [ns][grid_per_partic]
 //   <out>_obs0.txt calc_properties(): Upe Ubond Ptens... per-style energies
 //   <out>_xN.bin / <out>_fN.bin after N steps of forces(); Integrate_2(); update_pairstyles()
-// Options: -in <script> -out <prefix> [-steps N] [-nonoise]
+//   -nlist rc group: an NList (nlist.cu:13-112) of that group built on the initial positions:
+//   <out>_cell.bin d_particle_cell int [ns]; <out>_ncount.bin d_neigh_count int [ns];
+//   <out>_neigh.bin d_neigh_inds int [ns][CELL_MAX]; <out>_nlist.txt CELL_MAX total_ncells
+//   (the caller checks on the host first that no cell or row overflows CELL_MAX: the reference
+//   kernels do not bound their writes)
+// Options: -in <script> -out <prefix> [-steps N] [-nonoise] [-ninds K] [-nlist rc group]
+//   -ninds K dumps the stencils of the first K beads only (large systems)
 // Test infrastructure only (it links the reference build); nothing in the product uses it.
 #define MAIN
 #include "globals.h"
@@ -44,24 +50,45 @@ static void dump_obs(const std::string& name) {
 
 int main(int argc, char** argv) {
   std::string out = "ref";
+  std::string nl_group;
+  float nl_rc = 0.0f;
   int nsteps = 0, nonoise = 0;
+  long long ninds = -1;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     if (a == "-in" && i + 1 < argc) input_file = argv[++i];
     else if (a == "-out" && i + 1 < argc) out = argv[++i];
     else if (a == "-steps" && i + 1 < argc) nsteps = atoi(argv[++i]);
     else if (a == "-nonoise") nonoise = 1;
+    else if (a == "-ninds" && i + 1 < argc) ninds = atoll(argv[++i]);
+    else if (a == "-nlist" && i + 2 < argc) {
+      nl_rc = (float)atof(argv[++i]);
+      nl_group = argv[++i];
+    }
   }
   initialize();
   if (nonoise) noise_mag = 0.0f;
   step = 0;
   dump(out + "_x0.bin", d_x, sizeof(float) * ns * Dim);
+  if (!nl_group.empty()) {
+    NList nl;
+    nl.Initialize(nl_rc, nl_group);
+    nl.BuildNList();
+    cudaDeviceSynchronize();
+    dump(out + "_cell.bin", nl.d_particle_cell, sizeof(int) * ns);
+    dump(out + "_ncount.bin", nl.d_neigh_count, sizeof(int) * ns);
+    dump(out + "_neigh.bin", nl.d_neigh_inds, sizeof(int) * (size_t)ns * nl.CELL_MAX);
+    FILE* f = fopen((out + "_nlist.txt").c_str(), "w");
+    fprintf(f, "%d %d\n", nl.CELL_MAX, nl.total_ncells);
+    fclose(f);
+  }
   forces();
   cudaDeviceSynchronize();
   dump(out + "_f0.bin", d_f, sizeof(float) * ns * Dim);
   dump(out + "_rho0.bin", d_all_rho, sizeof(float) * (size_t)ntypes * M);
-  dump(out + "_inds.bin", d_grid_inds, sizeof(int) * (size_t)ns * grid_per_partic);
-  dump(out + "_w.bin", d_grid_W, sizeof(float) * (size_t)ns * grid_per_partic);
+  const size_t nst = (ninds >= 0 && ninds < ns) ? (size_t)ninds : (size_t)ns;
+  dump(out + "_inds.bin", d_grid_inds, sizeof(int) * nst * grid_per_partic);
+  dump(out + "_w.bin", d_grid_W, sizeof(float) * nst * grid_per_partic);
   calc_properties();
   dump_obs(out + "_obs0.txt");
   for (step = 1; step <= nsteps; step++) {

@@ -75,6 +75,52 @@ def test_driver_outputs_and_step0(tmp_path, kind):
     assert len(sk) == M - 1 and len(sk[0].split()) == 7
 
 
+@pytest.mark.parametrize("kind", ["neutral", "charged"])
+def test_read_resume_restarts_from_a_trajectory_frame(tmp_path, kind):
+    """read_resume (config_utils.cu:405-454) takes positions from a trajectory frame: a run
+    resumed from the step-3 frame of another run starts from those positions (its step-0 frame
+    prints them again, its step-0 energies are the oracle's at them).  On the charged frame the
+    reference program reads the same files to the same step-0 line; on a 3-D frame without
+    charges its reader misparses (its "%f " format swallows the newline and the next line's first
+    characters), so there only the oracle is compared."""
+    s = small_diblock(3, 1) if kind == "neutral" else charged_system()
+    a = tmp_path / "a"
+    a.mkdir()
+    setup_dir(a, s, steps=3)
+    run(EXE, a)
+    frame = [f for st, f in traj_frames(a / "traj.lammpstrj") if st == 3][0]
+    text = "ITEM: TIMESTEP\n" + frame
+    rows = [l.split() for l in frame.strip().split("\n")[8:]]
+    x3 = np.array([[float(v) for v in r[3:6]] for r in rows], np.float32)
+    assert x3.shape == (s.ns, 3)
+    outs = {}
+    for exe, sub in ((EXE, "b"), (REF, "c")):
+        if not os.path.exists(exe) or (sub == "c" and kind == "neutral"):
+            continue
+        d = tmp_path / sub
+        d.mkdir()
+        (d / "resume.lammpstrj").write_text(text)
+        setup_dir(d, s, steps=2, extra=["read_resume resume.lammpstrj"])
+        run(exe, d)
+        outs[sub] = d
+    b = outs["b"]
+    f0 = traj_frames(b / "traj.lammpstrj")[0]
+    assert f0[0] == 0 and f0[1].split("\n")[8:] == frame.split("\n")[8:]
+    assert "read_resume resume.lammpstrj" in open(b / "NEED_A_NAME.input").read()
+    _, rb = read_data_dat(b / "data.dat")
+    s.x = x3
+    o = oracle.Oracle(s)
+    o.forces(s.x, 0)
+    ob = o.observables(s.x)
+    assert rb[0][1] == pytest.approx(ob["upe"], rel=2e-5)
+    assert rb[0][2] == pytest.approx(ob["ubond"], rel=2e-5)
+    if "c" in outs:
+        _, rc = read_data_dat(outs["c"] / "data.dat")
+        # the reference sums in FP32 on the host: near-zero off-diagonal pressures carry its noise
+        np.testing.assert_allclose(rb[0], rc[0], rtol=5e-5, atol=1e-5 * np.abs(rc[0][3:6]).max())
+        assert open(b / "NEED_A_NAME.input").read() == open(outs["c"] / "NEED_A_NAME.input").read()
+
+
 def test_driver_matches_reference_program(tmp_path):
     """Same files through both programs: identical step-0 trajectory text, step-0 data.dat line
     and rho files within FP32 print precision."""

@@ -148,6 +148,52 @@ def test_group_integrators_move_only_their_type():
     assert not moved[s.types == 0].any() and moved[s.types == 1].all()
 
 
+GROUP_LISTS = {
+    # Integrate_2 runs every integrator of the input in order on its group (integrator.cu:24-39,
+    # group.cu:44-60); a bead in two groups is moved twice with the step's forces
+    "gjf_type1_em_type2": [(tild.INTEGRATOR_GJF, 0), (tild.INTEGRATOR_EM, 1)],
+    "em_all_em_type2": [(tild.INTEGRATOR_EM, -1), (tild.INTEGRATOR_EM, 1)],
+    "gjf_all_em_type1": [(tild.INTEGRATOR_GJF, -1), (tild.INTEGRATOR_EM, 0)],
+}
+
+
+@pytest.mark.parametrize("name", sorted(GROUP_LISTS))
+def test_group_integrator_positions_match_oracle(name):
+    """Positions of type-group and mixed integrator lists against the oracle: one step with
+    matched Philox noise, then five noise-off steps."""
+    s = small_diblock(3, 1)
+    s.integrators = GROUP_LISTS[name]
+    L = np.array(s.box[:3], np.float32)
+
+    def dist(a, b):
+        d = a - b
+        d -= L * np.round(d / L)
+        return float(np.abs(d).max())
+
+    x, xo, nz = s.x.copy(), s.x.copy(), np.zeros_like(s.x)
+    o = oracle.Oracle(s)
+    o.step(x, xo, nz, 1, True)
+    with tild.Context(s) as c:
+        c.step(1)
+        gx, gxo, gnz = c.get_state()
+    assert dist(gx, x) < 2e-5
+    np.testing.assert_allclose(gnz, nz, rtol=2e-5, atol=2e-6)
+    s.noise_mag = 0.0
+    x, xo, nz = s.x.copy(), s.x.copy(), np.zeros_like(s.x)
+    o = oracle.Oracle(s)
+    for k in range(1, 6):
+        o.step(x, xo, nz, k, False)
+    with tild.Context(s) as c:
+        c.step(5)
+        gx, _, _ = c.get_state()
+    assert dist(gx, x) < 1e-4
+    # beads outside every group stay where they were
+    covered = np.zeros(s.ns, bool)
+    for _, grp in s.integrators:
+        covered |= (s.types == grp) if grp >= 0 else True
+    assert np.array_equal(gx[~covered], s.x[~covered])
+
+
 def test_ten_steps_track_oracle_without_noise():
     s = small_diblock(3, 1)
     s.noise_mag = 0.0

@@ -67,3 +67,34 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     max_beads = 4096 * 256  # TILD_NOALLOC_MAX_BEADS
     st = f(dummy, dummy, dummy, dummy, max_beads + 1, 3, box, 1, one, one, dummy, None)
     assert st == tild.ERR_BAD_INPUT
+
+
+@pytest.mark.parametrize("fault", ["negative_partner", "partner_past_end", "bond_count"])
+def test_noalloc_corrupt_topology_gives_nan_energy(fault):
+    """A partner id or bond count out of range poisons the energy instead of giving a plausible
+    wrong number (a negative partner would otherwise be skipped by the j < i test)."""
+    torch = pytest.importorskip("torch")
+    s = small_diblock(3, 1)
+    nb = np.ascontiguousarray(s.n_bonds, np.int32).copy()
+    bt = np.ascontiguousarray(s.bonded_to, np.int32).copy()
+    i = int(np.nonzero(nb > 0)[0][5])
+    if fault == "negative_partner":
+        bt[i, 0] = -3
+    elif fault == "partner_past_end":
+        bt[i, 0] = s.ns + 7
+    else:
+        nb[i] = 4
+    dev = torch.device("cuda:0")
+    d_x = torch.from_numpy(np.ascontiguousarray(s.x)).to(dev)
+    d_nb = torch.from_numpy(nb).to(dev)
+    d_bt = torch.from_numpy(bt).to(dev)
+    d_by = torch.from_numpy(np.ascontiguousarray(s.bond_type, np.int32)).to(dev)
+    box = (C.c_float * 3)(*[float(v) for v in s.box[:3]])
+    bk = (C.c_float * len(s.bond_k))(*s.bond_k)
+    br = (C.c_float * len(s.bond_req))(*s.bond_req)
+    d_out = torch.zeros(7, dtype=torch.float64, device=dev)
+    st = _entry()(d_x.data_ptr(), d_nb.data_ptr(), d_bt.data_ptr(), d_by.data_ptr(), s.ns, 3, box, len(s.bond_k), bk,
+                  br, d_out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert st == tild.OK
+    torch.cuda.synchronize()
+    assert np.isnan(d_out.cpu().numpy()[0])
