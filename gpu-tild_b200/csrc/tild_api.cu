@@ -967,7 +967,7 @@ void get_tune(const tild_ctx* c, tild_tune* t) {
 
 int set_tune(tild_ctx* c, const tild_tune* t) {
   if (!t || (t->spread_mode != TILD_SPREAD_TILED && t->spread_mode != TILD_SPREAD_DIRECT) || t->spread_cap < 1024 ||
-      t->spread_cap > 12288 || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
+      t->spread_cap > 12288 || (t->spread_cap & 3) || t->sort_interval < 0 || t->fft_streams < 0 || t->fft_streams > 8 ||
       t->gather_mode < TILD_GATHER_DIRECT || t->gather_mode > TILD_GATHER_BOX || t->gather_cap < 1024 ||
       t->gather_cap > 3072 || t->field_layout < TILD_FIELD_LINEAR || t->field_layout > TILD_FIELD_BRICK ||
       (t->field_layout == TILD_FIELD_BRICK && c->D != 3) || t->fft_pipeline < 0 || t->fft_pipeline > 2 ||

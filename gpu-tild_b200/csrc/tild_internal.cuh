@@ -326,12 +326,12 @@ __device__ __forceinline__ void spline_w(float gdx, float H, float* W) {
   }
 }
 
-// Grid index and weights of one bead along one axis (device_grid_utils.cu:256-266): even
-// orders use the nearest node, odd orders the containing cell; base = first stencil node.
+// Grid index of one bead along one axis (device_grid_utils.cu:256-266): even orders use the
+// nearest node, odd orders the containing cell; returns the first stencil node and sets gdx, the
+// offset from that node or cell centre that the spline weights take.
 template <int P>
-__device__ __forceinline__ int axis_base(float xj, float dxj, float* W) {
+__device__ __forceinline__ int axis_index(float xj, float dxj, float& gdx) {
   int gi;
-  float gdx;
   if (P % 2 == 0) {
     gi = (int)((xj + 0.5f * dxj) / dxj);
     gdx = xj - (float)gi * dxj;
@@ -339,8 +339,16 @@ __device__ __forceinline__ int axis_base(float xj, float dxj, float* W) {
     gi = (int)(xj / dxj);
     gdx = xj - ((float)gi + 0.5f) * dxj;
   }
-  spline_w<P>(gdx, dxj, W);
   return gi - P / 2;
+}
+
+// Grid index and weights of one bead along one axis.
+template <int P>
+__device__ __forceinline__ int axis_base(float xj, float dxj, float* W) {
+  float gdx;
+  const int b = axis_index<P>(xj, dxj, gdx);
+  spline_w<P>(gdx, dxj, W);
+  return b;
 }
 
 // Periodic index with the reference's single conditional wrap; anything still outside the

@@ -129,7 +129,7 @@ __device__ __forceinline__ void spread_global_kbits(const float (&W)[3][P + 1], 
 template <int D, int P, bool CH>
 __device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], int t, float q, const SysDev& sd,
                                                unsigned long long* __restrict__ rho_fx, int cap, int* status) {
-  extern __shared__ int smi[];
+  extern __shared__ __align__(16) int smi[];  // the box: cap words, cap a multiple of 4
   __shared__ int s_g0[3], s_min[3], s_max[3];
   __shared__ int s_row[kMaxRows];  // row offsets in one channel (grids hold fewer than 2^31 points)
   const Geom g = sd.g;
@@ -144,11 +144,12 @@ __device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], in
     }
   }
   __syncthreads();
-  float W[3][P + 1];
+  // only the per-axis spline offsets live across the box barriers; the weights come after them
+  float gd[3] = {0.f, 0.f, 0.f};
   int rel[3] = {0, 0, 0};
   if (ok) {
 #pragma unroll
-    for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_base<P>(xs[d], g.dx[d], W[d]) - s_g0[d], g.nx[d]);
+    for (int d = 0; d < D; d++) rel[d] = fold_rel(axis_index<P>(xs[d], g.dx[d], gd[d]) - s_g0[d], g.nx[d]);
   }
   int mn[3], ext[3];
   long long vol;
@@ -159,9 +160,15 @@ __device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], in
   const bool qc = CH && C && q != 0.f;
   if (vol * nch <= cap && ext[0] <= 64 && ext[1] * ext[2] <= kMaxRows) {
     const int tot = (int)vol * nch;
-    for (int k = threadIdx.x; k < tot; k += blockDim.x) smi[k] = 0;
+    {  // clear with 16-byte stores (the box buffer holds cap words, cap a multiple of 4)
+      int4* s4 = reinterpret_cast<int4*>(smi);
+      for (int k = threadIdx.x; k < (tot + 3) >> 2; k += blockDim.x) s4[k] = make_int4(0, 0, 0, 0);
+    }
     __syncthreads();
     if (ok) {
+      float W[3][P + 1];
+#pragma unroll
+      for (int d = 0; d < D; d++) spline_w<P>(gd[d], g.dx[d], W[d]);
       const float sc32 = ig * __int_as_float((127 + kbits) << 23);  // 2^kbits / gvol
       int* st = smi + (long long)t * vol;
       int* sq = smi + (long long)T * vol;
@@ -186,7 +193,7 @@ __device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], in
         }
     }
     __syncthreads();
-    // flush: one warp per box row (y, z) and channel, lanes along x; exact shift to the 2^32 grid
+    // row offsets of the box in one channel of the periodic grid
     const int rows_per = ext[1] * ext[2];
     for (int yz = threadIdx.x; yz < rows_per; yz += blockDim.x) {
       const int ly = yz % ext[1], lz = yz / ext[1];
@@ -194,34 +201,30 @@ __device__ __forceinline__ void cta_spread_box(bool ok, const float (&xs)[3], in
                              g.nx[1] * (D == 3 ? pmod(s_g0[2] + mn[2] + lz, g.nx[2]) : 0));
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    // flush: every thread takes box words tid, tid + 256, ... of each channel (all lanes busy);
+    // a word's row is k / ext0 by a multiply-high (exact: k < 2^26, ext0 >= 3), and each nonzero
+    // word is shifted exactly onto the 2^32 grid and added with one 64-bit RED
+    const int ex = ext[0];
+    const unsigned mul = 0xFFFFFFFFu / (unsigned)ex + 1u;  // ceil(2^32 / ex)
     const int bx = pmod(s_g0[0] + mn[0], g.nx[0]);
-    int xoff[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      int xg = bx + lane + 32 * k;
-      while (xg >= g.nx[0]) xg -= g.nx[0];
-      xoff[k] = xg;
-    }
     const int sh = 32 - kbits;
     for (int ch = 0; ch < nch; ch++) {
       const int* sch = smi + (long long)ch * vol;
       unsigned long long* gch = rho_fx + ch * M;
-      for (int yz = warp; yz < rows_per; yz += nwarps) {
-        const int* srow = sch + (long long)yz * ext[0];
-        unsigned long long* grow = gch + s_row[yz];
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int lx = lane + 32 * k;
-          if (lx < ext[0]) {
-            const int v = srow[lx];
-            if (v != 0) atomicAdd(grow + xoff[k], (unsigned long long)((long long)v << sh));
-          }
-        }
+      for (int k = threadIdx.x; k < (int)vol; k += blockDim.x) {
+        const int v = sch[k];
+        if (v == 0) continue;
+        const int row = (int)__umulhi((unsigned)k, mul);
+        int xg = bx + (k - row * ex);
+        while (xg >= g.nx[0]) xg -= g.nx[0];
+        atomicAdd(gch + s_row[row] + xg, (unsigned long long)((long long)v << sh));
       }
     }
   } else if (ok) {
     // the box does not fit: the same 2^kbits contributions, added to the global grid directly
+    float W[3][P + 1];
+#pragma unroll
+    for (int d = 0; d < D; d++) spline_w<P>(gd[d], g.dx[d], W[d]);
     int idx[3][P + 1];
 #pragma unroll
     for (int d = 0; d < D; d++)

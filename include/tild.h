@@ -281,7 +281,7 @@ enum { TILD_GATHER_DIRECT = 0, TILD_GATHER_BOX = 1 };
 enum { TILD_FIELD_LINEAR = 0, TILD_FIELD_BRICK = 1 };
 typedef struct tild_tune {
   int32_t spread_mode;    /* order >= 2: shared-memory box per 256 beads (TILED) or 64-bit global atomics (DIRECT) */
-  int32_t spread_cap;     /* shared box of the tiled spread, 32-bit words, 1024..12288 */
+  int32_t spread_cap;     /* shared box of the tiled spread, 32-bit words, 1024..12288, a multiple of 4 */
   int32_t sort_interval;  /* steps between spatial sorts; 0 = never (only when the context sorts) */
   int32_t fft_streams;    /* auxiliary streams the per-grid-shape FFTs are spread over (0..8) */
   int32_t gather_mode;    /* order >= 2: stencil nodes read from global memory (DIRECT) or from a shared

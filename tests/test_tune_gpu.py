@@ -39,6 +39,7 @@ def run(s, tune=None, steps=70):
     {"spread_ahead": 1},                  # the gather spreads for the next step (shared box)
     {"spread_ahead": 1, "spread_mode": tild.SPREAD_DIRECT},
     {"spread_ahead": 1, "spread_cap": 1024},
+    {"spread_cap": 3072, "field_layout": tild.FIELD_BRICK},
 ])
 def test_every_setting_gives_the_same_trajectory(tune):
     s = p3_system()
