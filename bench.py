@@ -19,12 +19,21 @@ Arms:
                     the same workload.  When the reference's own CUDA build is present
                     (oracle/_ref/gpu-tild) its particle-steps/s on this GPU is added as
                     "reference_cuda".
+The default line (workload blend) also carries, as extra keys on their own configurations:
+  "ensemble": the 256-system batch (K steps, autotuned schedule) against the same systems run
+              one at a time through libtild and through the reference build, with its roofline;
+  "serving":  the Poisson stream of ensemble-distributed jobs at 50 jobs/s (overloaded: it offers
+              more particle-steps than one B200 sustains) and at a rate below capacity, with p50/p99
+              job latency, aggregate particle-steps/s and the ratio to the jobs run alone.
+--no-extras leaves them out.  Exactly K = --steps steps are timed: whole CUDA-graph periods
+plus direct launches for any remainder.
 Multi-GPU (torchrun, N > 1): one independent replica per GPU (systems do not exchange
 anything), timing = max over ranks, value = total particle-steps of all ranks / that time.
 """
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import shutil
@@ -66,37 +75,42 @@ def ensemble(n: int = 256):
     return [ts.ensemble_member(i) for i in range(n)]
 
 
-def run_ensemble(args):
+def ensemble_leg(grp, args) -> dict:
     """Batched ensemble: 256 independent diblock systems (box L ~ U(12, 24) snapped to dx = 0.5,
     grids 24^3..48^3, N ~ U{10..40}, f_A ~ U(0.3, 0.7), chi N ~ U(10, 30), rho0 = 5) advanced
-    together, against the same systems run one at a time (a sample of them, scaled)."""
-    grp = tild_dist.Group(backend="nccl")
+    together for exactly args.steps steps, against the same systems run one at a time (a sample
+    of them, scaled by bead counts), through libtild and through the reference build."""
     systems = ensemble(args.nsys)
     mine = tild_dist.shard([s.ns for s in systems], grp.rank, grp.world)
     local = [systems[i] for i in mine]
     B = tild.Batch(local, device=grp.local)
     schedule = None if args.no_tune else B.autotune(trial_steps=64)
-    period = int(grp.max(graph_period(B.get_tune())))  # the same step count on every rank
-    args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
-    B.step(-(-args.warmup * 32 // period) * period)
+    steps = args.steps
+    B.step(max(args.warmup, graph_period(B.get_tune())))
     B.sync()
     grp.barrier()
-    with ClockSampler(grp.local) as clk, nvtx_range("timed"):
-        ms = B.time_steps(args.steps)
+    with ClockSampler(grp.local) as clk, nvtx_range("timed_ensemble"):
+        ms = B.time_steps(steps)
     ms = grp.max(ms)
-    tot = grp.sum(sum(s.ns for s in local)) * args.steps
+    tot = grp.sum(sum(s.ns for s in local)) * steps
     value = tot / (ms / 1e3)
-    prof = B.profile_steps(args.steps)
+    prof = B.profile_steps(steps)
     B.close()
-    out = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": grp.world,
-           "steps": args.steps, "warmup": args.warmup * 32, "ms_per_step": ms / args.steps, "higher_is_better": True,
-           "scaling": "weak" if grp.world == 1 else "strong", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic (seeded random-walk chains)",
+    Sall = ensemble_bytes(systems)
+    dom = max(prof, key=lambda k: prof[k])
+    peak, peak_kind = hbm_peak()
+    out = {"value": value, "unit": "particle-steps/s", "steps": steps, "ms_per_step": ms / steps,
            "config": {"workload": f"ensemble_{args.nsys}_diblock_24^3-48^3_gaussian_p1_GJF",
                       "systems": args.nsys, "beads_total": sum(s.ns for s in systems),
                       "grid_points_total": int(sum(np.prod(s.nx) for s in systems)), "parallelism": f"shards{grp.world}",
                       "schedule": schedule},
-           "clocks": clk.summary(), "stages_ms_per_step": {k: v / args.steps for k, v in prof.items()}}
+           "clocks": clk.summary(), "stages_ms_per_step": {k: v / steps for k, v in prof.items()},
+           "roofline": {"bound": "hbm", "kernel": dom, "achieved": Sall[dom] / (prof[dom] / steps / 1e3) / 1e9
+                        if prof[dom] > 0 else 0.0, "peak": peak, "unit": "GB/s",
+                        "frac": Sall[dom] / (prof[dom] / steps / 1e3) / 1e9 / peak if prof[dom] > 0 else 0.0,
+                        "peak_source": peak_kind, "algorithmic_bytes_per_launch": Sall[dom]},
+           "step_roofline": {"algorithmic_bytes_per_step": Sall["step"],
+                             "frac": Sall["step"] / (ms / steps / 1e3) / 1e9 / peak}}
     if grp.rank == 0 and not args.no_serial:
         # one at a time: every 16th system alone, scaled to all systems by their bead counts
         sample = list(range(0, args.nsys, 16))
@@ -104,19 +118,19 @@ def run_ensemble(args):
         for i in sample:
             s = systems[i]
             with tild.Context(s, device=grp.local) as c:
-                c.step(args.warmup * 32)
-                t_serial += c.time_steps(args.steps) / 1e3
+                c.step(max(args.warmup, 32))
+                t_serial += c.time_steps(steps) / 1e3
                 ns_sample += s.ns
-        serial_value = ns_sample * args.steps / t_serial
+        serial_value = ns_sample * steps / t_serial
         out["serial"] = {"value": serial_value, "unit": "particle-steps/s",
-                         "sample": f"{len(sample)} of {args.nsys} systems, each alone for {args.steps} steps"}
+                         "sample": f"{len(sample)} of {args.nsys} systems, each alone for {steps} steps"}
         out["batched_over_serial"] = value / serial_value
         if not args.no_reference_cuda:
             # the reference's own build, one system per process as it runs them
             ref_sample = sample[::4]
             t_ref, ns_ref = 0.0, 0
             for i in ref_sample:
-                r = reference_cuda(systems[i], "ensemble_member")
+                r = reference_cuda(systems[i], "ensemble_member", pairs=1)
                 if r is None or "unavailable" in r:
                     t_ref = None
                     break
@@ -129,44 +143,64 @@ def run_ensemble(args):
                     "sample": f"{len(ref_sample)} of {args.nsys} systems, each a separate run of the reference build "
                               "(per-step time from two run lengths)"}
                 out["batched_over_reference_serial"] = value / ref_value
+    return out
+
+
+def ensemble_bytes(systems) -> dict:
+    """Algorithmic bytes of one launch of each stage over all systems, and of one whole step."""
+    tot = collections.Counter()
+    for s in systems:
+        tot.update(stage_bytes(s))
+        tot["step"] += step_bytes(s)
+    return dict(tot)
+
+
+def run_ensemble(args):
+    grp = tild_dist.Group(backend="nccl")
+    leg = ensemble_leg(grp, args)
     grp.close()
     if grp.rank == 0:
+        out = {"metric": "particle-steps/s", "value": leg["value"], "unit": "particle-steps/s", "n_gpus": grp.world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["ms_per_step"], "higher_is_better": True,
+               "scaling": "weak" if grp.world == 1 else "strong", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded random-walk chains)"}
+        out.update({k: v for k, v in leg.items() if k not in out})
         print(json.dumps(out))
 
 
-def run_serving(args):
-    """Serving: a seeded Poisson stream (mean --rate jobs/s) of jobs drawn from the batched-ensemble
-    distribution, each --job-steps steps returning its energy trace and avg_sk, served by
-    continuous batching over a slot pool (--slots-per-edge slots for each grid edge 24..48).
-    value: aggregate particle-steps/s of all jobs over the span from the first arrival to the
-    last completion; latency percentiles are arrival -> results on the host.  Against: the same
-    jobs run one at a time alone (a sample of them, each for all its steps)."""
+def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True) -> dict:
+    """Serving: a seeded Poisson stream (mean `rate` jobs/s) of `njobs` jobs drawn from the
+    batched-ensemble distribution, each --job-steps steps returning its energy trace and avg_sk,
+    served by continuous batching over slot pools (--slots-per-edge initial slots for each grid
+    edge 24..48, more grown on demand inside the HBM budget).  value: aggregate particle-steps/s
+    of all jobs over the span from the first arrival to the last completion; latency percentiles
+    are arrival -> results on the host.  Against: the same jobs run one at a time alone (a sample
+    of them, each for all its steps, set-up included)."""
     import tild_serve as sv
-    grp = tild_dist.Group(backend="nccl")
-    jobs_all = sv.poisson_jobs(args.jobs, args.rate, steps=args.job_steps)
+    jobs_all = sv.poisson_jobs(njobs, rate, steps=args.job_steps)
     mine = [j for k, j in enumerate(jobs_all) if k % grp.world == grp.rank]
     # each rank replays its share of the stream: arrivals keep their absolute times
     edges = {g: args.slots_per_edge for g in ts.ensemble_grid_edges()}
-    with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch,
-                   tune=not args.no_tune) as srv:
-        pool_bytes, nslots, schedule = srv.pool_bytes, srv.nslots, srv.schedule
+    with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch, tune=not args.no_tune,
+                   grow=not args.no_grow, group_slots=args.group_slots) as srv:
+        pool0, nslots, schedule = srv.pool_bytes, srv.nslots, srv.schedule
         grp.barrier()
         res = srv.run(mine, clock="wall")
         stepping_s, work_stepping = srv.stepping_s, srv.work_done
+        grown, peak_bytes = srv.pools_grown, srv.peak_bytes
     rows = grp.gather_lists([(r.job_id, r.ns, r.steps, r.arrival, r.admitted, r.finished) for r in res])
     rows.sort()
     results = [sv.JobResult(j, ns, 0, st, a, admitted=ad, finished=f) for j, ns, st, a, ad, f in rows]
     summ = sv.latency_summary(results)
     work = sum(r.ns * r.steps for r in results)
-    offered = args.rate * work / len(results)
-    out = {"metric": "particle-steps/s (aggregate, served jobs); p50/p99 job latency", "value":
-           summ["aggregate_particle_steps_per_s"], "unit": "particle-steps/s", "n_gpus": grp.world,
-           "steps": args.job_steps, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32", "data": "synthetic (seeded random-walk chains, seeded Poisson arrivals)",
-           "config": {"workload": f"serving_poisson{args.rate:g}_{args.jobs}jobs_{args.job_steps}steps",
-                      "slots": nslots * grp.world, "slots_per_edge": args.slots_per_edge, "epoch_steps": args.epoch,
-                      "hbm_budget_gb": args.hbm_budget / 1e9, "pool_gb_per_gpu": pool_bytes / 1e9,
-                      "schedule": schedule,
+    offered = rate * work / len(results)
+    out = {"metric": "particle-steps/s (aggregate, served jobs); p50/p99 job latency",
+           "value": summ["aggregate_particle_steps_per_s"], "unit": "particle-steps/s",
+           "config": {"workload": f"serving_poisson{rate:g}_{njobs}jobs_{args.job_steps}steps",
+                      "initial_slots": nslots * grp.world, "slots_per_edge": args.slots_per_edge,
+                      "grown_pools_rank0": grown, "group_slots": args.group_slots, "epoch_steps": args.epoch,
+                      "hbm_budget_gb": args.hbm_budget / 1e9, "initial_pool_gb_per_gpu": pool0 / 1e9,
+                      "peak_pool_gb_rank0": peak_bytes / 1e9, "schedule": schedule,
                       "parallelism": f"replicas{grp.world}"},
            "latency": summ,
            "offered_particle_steps_per_s": offered,
@@ -174,9 +208,8 @@ def run_serving(args):
            "stepping_throughput_rank0": {
                "value": work_stepping / stepping_s if stepping_s > 0 else None, "unit": "particle-steps/s",
                "note": "particle-steps the jobs advanced / wall time of the stepping calls: the batched engine's rate "
-                       "inside the request loop; the aggregate value also spans the stream's ramp-up and drain and "
-                       "the queueing of grid shapes whose slots are full"}}
-    if grp.rank == 0 and not args.no_serial:
+                       "inside the request loop; the aggregate value also spans the stream's ramp-up and drain"}}
+    if grp.rank == 0 and serial and not args.no_serial:
         sample = jobs_all[:: max(1, len(jobs_all) // args.serial_sample)][:args.serial_sample]
         t_serial, w_serial, lat = 0.0, 0, []
         for j in sample:
@@ -194,8 +227,18 @@ def run_serving(args):
                          "sample": f"{len(sample)} of {len(jobs_all)} jobs, each alone for all its steps "
                                    "(set-up included)"}
         out["served_over_serial"] = out["value"] / out["serial"]["value"]
+    return out
+
+
+def run_serving(args):
+    grp = tild_dist.Group(backend="nccl")
+    leg = serving_leg(grp, args, args.rate, args.jobs)
     grp.close()
     if grp.rank == 0:
+        out = {"metric": leg["metric"], "value": leg["value"], "unit": "particle-steps/s", "n_gpus": grp.world,
+               "steps": args.job_steps, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32", "data": "synthetic (seeded random-walk chains, seeded Poisson arrivals)"}
+        out.update({k: v for k, v in leg.items() if k not in out})
         print(json.dumps(out))
 
 
@@ -323,9 +366,9 @@ def run_ours(args):
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
     schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
-    period = int(grp.max(graph_period(ctx.get_tune())))  # the same step count on every rank
-    args.steps = -(-args.steps // period) * period   # whole graph periods: no direct-launch remainder
-    ctx.step(args.warmup)
+    # warm-up: the requested steps, then whole graph periods (every graph of the timed region is
+    # captured before it; a remainder shorter than a period runs as direct launches)
+    ctx.step(args.warmup + graph_period(ctx.get_tune()))
     ctx.sync()
     grp.barrier()
     with ClockSampler(local) as clk, nvtx_range("timed"):
@@ -361,7 +404,7 @@ def run_ours(args):
         n = min(log_freq, e2e_steps - done)
         ctx.step(n)
         done += n
-        if done % log_freq == 0:
+        if done % log_freq == 0 or done == e2e_steps:   # a record every 128 steps and at the end
             ctx.observables()
             obs_reads += 1
     ctx.snapshot_wait(ctx.snapshot_async(x_out.array, None))   # final positions to the host
@@ -372,8 +415,8 @@ def run_ours(args):
     d2h = s.ns * s.dim * 4 + obs_reads * obs_bytes
     e2e = {"value": per_rank * ws / e2e_s, "unit": "particle-steps/s",
            "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
-           "note": "public C ABI from page-locked host arrays: upload positions, K steps, observables every "
-                   "128 steps, download positions"}
+           "note": "public C ABI from page-locked host arrays: upload positions, K steps, an FP64 observables "
+                   "record every 128 steps and after the last step, download positions"}
 
     out = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
@@ -398,6 +441,12 @@ def run_ours(args):
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(s, args)
     ctx.close()
+    if args.workload == "blend" and not args.no_extras:
+        out["ensemble"] = ensemble_leg(grp, args)
+        out["serving"] = [serving_leg(grp, args, 50.0, args.jobs),
+                          serving_leg(grp, args, args.subsat_rate, args.subsat_jobs, serial=False)]
+        if rank == 0 and "serial" in out["serving"][0]:
+            out["serving"][1]["served_over_serial"] = out["serving"][1]["value"] / out["serving"][0]["serial"]["value"]
     grp.close()
     if rank == 0:
         print(json.dumps(out))
@@ -424,32 +473,38 @@ def cpu_baseline(s, args, target_s: float = 20.0):
                       f"(oracle/tild_oracle.c, FP64, OpenMP {cores} threads)"}
 
 
-def reference_cuda(s, wname, steps=None):
+def reference_cuda(s, wname, steps=None, pairs: int = 3):
     """The reference program built from its own sources (oracle/_ref/gpu-tild) on this GPU:
-    per-step time = difference of wall times of two runs that differ only in max_steps.  The
-    longer run is sized (about 3 s of stepping at the reference's C2 rate per bead, at least 100
-    steps) so the difference dominates the run-to-run spread of process start-up."""
+    per-step time = difference of wall times of two runs that differ only in max_steps, so setup
+    and output cancel.  The longer run is sized (about 3 s of stepping at the reference's rate
+    per bead, at least 100 steps) so the difference dominates the spread of process start-up;
+    `pairs` such pairs are timed and the median is reported with the range."""
     if steps is None:
         extra = int(min(20000, max(100, 3.0 / (s.ns * 4e-9))))
         steps = (20, 20 + extra)
     exe = os.path.join(ROOT, "oracle", "_ref", "gpu-tild")
     if not os.path.exists(exe):
         return None
-    times = []
+    per = []
     with tempfile.TemporaryDirectory() as td:
         ts.write_data_file(os.path.join(td, "input.data"), s)
-        for n in steps:
-            ts.write_input_script(os.path.join(td, "input"), s, max_steps=n, log_freq=10 ** 8, binary_freq=0)
-            t0 = time.perf_counter()
-            r = subprocess.run([exe, "-in", "input"], cwd=td, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
-                               timeout=900)
-            times.append(time.perf_counter() - t0)
-            if r.returncode != 0:
-                return {"unavailable": f"reference build exited {r.returncode}"}
-    per_step = (times[1] - times[0]) / (steps[1] - steps[0])
+        for _ in range(pairs):
+            times = []
+            for n in steps:
+                ts.write_input_script(os.path.join(td, "input"), s, max_steps=n, log_freq=10 ** 8, binary_freq=0)
+                t0 = time.perf_counter()
+                r = subprocess.run([exe, "-in", "input"], cwd=td, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                                   timeout=900)
+                times.append(time.perf_counter() - t0)
+                if r.returncode != 0:
+                    return {"unavailable": f"reference build exited {r.returncode}"}
+            per.append((times[1] - times[0]) / (steps[1] - steps[0]))
+    per_step = float(np.median(per))
     return {"value": s.ns / per_step, "unit": "particle-steps/s", "ms_per_step": per_step * 1e3,
+            "ms_per_step_pairs": [p * 1e3 for p in per],
             "binary": "oracle/_ref/gpu-tild (unmodified reference sources, nvcc -arch=sm_100a -O3)",
-            "method": f"wall-time difference of {steps[1]}- and {steps[0]}-step runs (setup and output cancel)"}
+            "method": f"median over {pairs} pairs of the wall-time difference of {steps[1]}- and {steps[0]}-step runs "
+                      "(setup and output cancel)"}
 
 
 def run_reference(args):
@@ -484,7 +539,12 @@ def main():
     ap.add_argument("--jobs", type=int, default=300, help="serving: number of jobs in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: mean arrivals per second")
     ap.add_argument("--job-steps", type=int, default=5000)
-    ap.add_argument("--slots-per-edge", type=int, default=12)
+    ap.add_argument("--slots-per-edge", type=int, default=12, help="serving: initial slots per grid edge")
+    ap.add_argument("--group-slots", type=int, default=8, help="serving: slots of a pool grown on demand")
+    ap.add_argument("--no-grow", action="store_true", help="serving: fixed slots only")
+    ap.add_argument("--subsat-rate", type=float, default=4.0, help="serving: the below-capacity arrival rate")
+    ap.add_argument("--subsat-jobs", type=int, default=40)
+    ap.add_argument("--no-extras", action="store_true", help="blend line only (no ensemble and serving legs)")
     ap.add_argument("--epoch", type=int, default=128)
     ap.add_argument("--hbm-budget", type=float, default=80e9)
     ap.add_argument("--serial-sample", type=int, default=6)

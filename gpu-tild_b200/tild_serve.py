@@ -1,30 +1,36 @@
 """Continuous batching of TILD simulation jobs on one GPU.
 
 The reference runs one system per process (main.cu:47-290) and has no request loop; this module
-is the serving form layered on the batched engine.  A pool of slots is created once: each slot
-is a system of a slot batch (tild_batch_create_slots) with a fixed grid shape and a bead
-capacity, so its state stays resident in HBM.  The loop
+is the serving form layered on the batched engine.  Slots live in pools: a pool is one slot batch
+(tild_batch_create_slots), each slot a system with a fixed grid shape and a bead capacity, so its
+state stays resident in HBM.  The server starts with one pool of a fixed number of slots per grid
+edge; with grow=True, a job whose grid shape has no free slot gets a new pool of `group_slots`
+slots of that shape whenever the device footprint of all pools stays inside the HBM budget, and
+pools that have run no job for `idle_epochs` epochs are released.  Admission is therefore bounded
+by memory, not by a fixed number of slots per shape.  The loop
 
-  1. admits arrived jobs, first come first served, into free slots of their grid shape while the
-     pool's device footprint stays inside the HBM budget (tild_batch_load rebuilds the slot's
-     k-space tables, then topology and state are uploaded and the slot is activated with a
+  1. admits arrived jobs, first come first served, into free slots of their grid shape, growing
+     a pool for the shape when none is free and the budget allows (tild_batch_load rebuilds the
+     slot's k-space tables, then topology and state are uploaded and the slot is activated with a
      device-side stop at the job's step count);
-  2. advances every active slot by one epoch of `epoch` steps in one stepping call (CUDA graphs,
-     one launch per stage for all slots), so jobs admitted at different times overlap on the GPU;
+  2. advances every pool with an active slot by one epoch of `epoch` steps (CUDA graphs, one
+     launch per stage for all slots of a pool); pools step concurrently from worker threads, each
+     on its own stream, so jobs admitted at different times overlap on the GPU;
   3. evaluates the densities of every slot at its current positions (one force evaluation without a
      step; stopped slots hold their last positions) and records each running job's energy (FP64
      observables) and accumulates its avg_sk, so every record describes the state at its step;
   4. retires the jobs whose slots left the active set on the device (their last step ran inside
      the epoch), returning the energy trace and S(k) and freeing the slot for the queue.
 
-A job's result does not depend on what else runs: the spread is fixed point (order-independent),
-the noise is keyed by (bead id, step, seed), and every other kernel is per bead or per grid
-point of one system.  Only cuFFT's batched transforms could round differently with the batch
-size; the serving test bounds that.
+A job's result does not depend on what else runs or which pool holds it: the spread is fixed
+point (order-independent), the noise is keyed by (bead id, step, seed), and every other kernel is
+per bead or per grid point of one system.  Only cuFFT's batched transforms could round
+differently with the batch size; the serving test bounds that.
 """
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import dataclasses
 import math
 import time
@@ -94,55 +100,161 @@ def device_free_bytes(device: int) -> int:
     return int(free)
 
 
-class Server:
-    """A slot pool plus the request loop.
+def slot_bytes_estimate(g: int, capacity: int) -> int:
+    """Device bytes of one slot of grid edge g (diblock: two density channels, three gaussian
+    styles) from the engine's layout: per grid point and channel 8 (fixed-point) + 4 (density) +
+    12 (planar field) + 16 (float4 field) bytes and 32 bytes of half spectra, the multiplier and
+    virial tables, and about 100 bytes per bead of capacity.  Used when the footprint is not
+    measured on the device."""
+    M = g ** 3
+    return int(2 * 40 * M + 2 * 16 * M + 3 * 2 * M + 3 * 6 * 4 * M + 100 * capacity)
 
-    slots_per_edge: number of slots for each grid edge g (g^3 grids).
+
+class _Pool:
+    """One slot batch: its slots' grid edges, whether it was grown on demand, its device bytes."""
+
+    def __init__(self, pid: int, batch, edges: List[int], grown: bool, nbytes: int):
+        self.pid = pid
+        self.batch = batch
+        self.edges = list(edges)
+        self.grown = grown
+        self.nbytes = int(nbytes)
+        self.idle = 0                      # consecutive epochs with no job in any slot
+
+
+class Server:
+    """Slot pools plus the request loop.
+
+    slots_per_edge: slots of the initial pool for each grid edge g (g^3 grids).
     capacity_of(g): bead capacity of a slot of edge g.
-    template_of(g): a system of edge g that initialises the slot before its first job.
-    hbm_budget: bytes the pool may occupy on the device; creation fails beyond it.
+    template_of(g): a system of edge g that initialises a slot before its first job.
+    hbm_budget: bytes all pools may occupy on the device; the initial pool must fit, and pools
+      are grown only while the total stays inside it.
     epoch: steps per stepping call (a multiple of 32 keeps every call inside CUDA graphs).
+    grow: create a pool of `group_slots` slots for a grid shape whose slots are all busy while a
+      job of that shape waits and the budget allows; release grown pools idle for `idle_epochs`.
+    Slots are named by integers that stay unique for the server's lifetime.
     """
 
     def __init__(self, slots_per_edge: Dict[int, int], capacity_of: Callable[[int], int] = ts.ensemble_capacity,
                  template_of: Callable[[int], tild.System] = ts.ensemble_slot_template, device: int = 0,
                  hbm_budget: float = 80e9, epoch: int = 128, keep_positions: bool = False,
-                 measure_memory: bool = True, tune: bool = False):
+                 measure_memory: bool = True, tune: bool = False, grow: bool = False, group_slots: int = 4,
+                 idle_epochs: int = 2):
         self.device = device
         self.epoch = int(epoch)
         self.keep_positions = keep_positions
         self.hbm_budget = float(hbm_budget)
-        systems, caps, self.edge_of_slot = [], [], []
-        for g, n in sorted(slots_per_edge.items()):
-            tpl = template_of(g)
-            for _ in range(n):
-                systems.append(tpl)
-                caps.append(max(capacity_of(g), tpl.ns))
-                self.edge_of_slot.append(g)
-        free0 = device_free_bytes(device) if measure_memory else 0
-        self.batch = self._make_batch(systems, caps)
-        self.batch.sync()
-        self.pool_bytes = (free0 - device_free_bytes(device)) if measure_memory else 0
-        if self.pool_bytes > self.hbm_budget:
-            self.batch.close()
-            raise MemoryError(f"slot pool needs {self.pool_bytes / 1e9:.1f} GB, budget {self.hbm_budget / 1e9:.1f} GB")
-        # schedule chosen on the full pool (every slot holding its template system)
-        self.schedule = self.batch.autotune(trial_steps=64) if tune else None
-        for i in range(len(systems)):
-            self.batch.set_active(i, False)
+        self.capacity_of = capacity_of
+        self.template_of = template_of
+        self.measure_memory = measure_memory
+        self.grow = grow
+        self.group_slots = int(group_slots)
+        self.idle_epochs = int(idle_epochs)
+        self.pools: Dict[int, _Pool] = {}
+        self.slot_at: Dict[int, tuple] = {}          # slot -> (pool id, index in the pool)
         self.free: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
-        for i, g in enumerate(self.edge_of_slot):
-            self.free[g].append(i)
-        self.nslots = len(systems)
+        self.edges = set(slots_per_edge)
+        self._next_pid = 0
+        self._next_slot = 0
+        self.pools_grown = 0
+        self.pools_released = 0
+        self.peak_bytes = 0
+        edges = [g for g, n in sorted(slots_per_edge.items()) for _ in range(n)]
+        pool = self._new_pool(edges, grown=False)
+        if pool.nbytes > self.hbm_budget:
+            pool.batch.close()
+            raise MemoryError(f"slot pool needs {pool.nbytes / 1e9:.1f} GB, budget {self.hbm_budget / 1e9:.1f} GB")
+        # schedule chosen on the initial pool (every slot holding its template system); grown
+        # pools take it too, with their single grid shape's FFTs on the main stream
+        self.schedule = pool.batch.autotune(trial_steps=64) if tune else None
+        self._tune = pool.batch.get_tune() if tune else None
+        self._register(pool)
+        self.nslots = len(edges)
         self.epochs_run = 0
         self.stepping_s = 0.0     # wall time of the stepping calls and their force evaluation
         self.work_done = 0        # particle-steps the jobs advanced inside those calls
+        self._exec = concurrent.futures.ThreadPoolExecutor(max_workers=8)
+
+    @property
+    def pool_bytes(self) -> int:
+        return sum(p.nbytes for p in self.pools.values())
 
     def _make_batch(self, systems, caps):
         return tild.Batch(systems, device=self.device, capacity=caps)
 
+    def _new_pool(self, edges: List[int], grown: bool) -> _Pool:
+        systems, caps = [], []
+        for g in edges:
+            tpl = self.template_of(g)
+            systems.append(tpl)
+            caps.append(max(self.capacity_of(g), tpl.ns))
+        free0 = device_free_bytes(self.device) if self.measure_memory else 0
+        batch = self._make_batch(systems, caps)
+        batch.sync()
+        if self.measure_memory:
+            nbytes = free0 - device_free_bytes(self.device)
+        else:
+            nbytes = sum(slot_bytes_estimate(g, c) for g, c in zip(edges, caps))
+        pool = _Pool(self._next_pid, batch, edges, grown, nbytes)
+        self._next_pid += 1
+        return pool
+
+    def _register(self, pool: _Pool):
+        for i in range(len(pool.edges)):
+            pool.batch.set_active(i, False)
+        self.pools[pool.pid] = pool
+        for i, g in enumerate(pool.edges):
+            sid = self._next_slot
+            self._next_slot += 1
+            self.slot_at[sid] = (pool.pid, i)
+            self.free[g].append(sid)
+        self.peak_bytes = max(self.peak_bytes, self.pool_bytes)
+
+    def _release(self, pool: _Pool):
+        mine = {sid for sid, (pid, _) in self.slot_at.items() if pid == pool.pid}
+        for g in set(pool.edges):
+            self.free[g] = collections.deque(sid for sid in self.free[g] if sid not in mine)
+        for sid in mine:
+            del self.slot_at[sid]
+        del self.pools[pool.pid]
+        pool.batch.close()
+        self.pools_released += 1
+
+    def _try_grow(self, g: int, running: dict) -> bool:
+        """A pool of group_slots slots of edge g, if the budget allows (idle grown pools of other
+        shapes are released first when that makes room).  Returns whether slots were added."""
+        caps = [max(self.capacity_of(g), self.template_of(g).ns)] * self.group_slots
+        need = sum(slot_bytes_estimate(g, c) for c in caps)
+        known = [p for p in self.pools.values() if p.grown and p.edges[0] == g]
+        if known:
+            need = known[0].nbytes
+        if self.pool_bytes + need > self.hbm_budget:
+            busy = {self.slot_at[sid][0] for sid in running}
+            for p in sorted(self.pools.values(), key=lambda p: -p.idle):
+                if p.grown and p.pid not in busy and self.pool_bytes + need > self.hbm_budget:
+                    self._release(p)
+            if self.pool_bytes + need > self.hbm_budget:
+                return False
+        pool = self._new_pool([g] * self.group_slots, grown=True)
+        if self._tune is not None:
+            t = pool.batch.get_tune()
+            for f, _ in tild.Tune._fields_:
+                if f not in ("fft_streams", "fft_pipeline", "ms_per_step"):
+                    setattr(t, f, getattr(self._tune, f))
+            pool.batch.set_tune(t)
+        if self.pool_bytes + pool.nbytes > self.hbm_budget:
+            pool.batch.close()
+            return False
+        self._register(pool)
+        self.pools_grown += 1
+        return True
+
     def close(self):
-        self.batch.close()
+        self._exec.shutdown(wait=True)
+        for p in list(self.pools.values()):
+            p.batch.close()
+        self.pools.clear()
 
     def __enter__(self):
         return self
@@ -150,32 +262,56 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
+    def _b(self, slot: int):
+        pid, i = self.slot_at[slot]
+        return self.pools[pid].batch, i
+
     # ---------------------------------------------------------------------------------------
     def checkpoint(self, slot: int, job: Job, r: JobResult, epochs_run: int = 0) -> Checkpoint:
         """Takes the full state of the job in `slot` off the GPU and frees the slot."""
-        x, xo, nz = self.batch.get_state(slot)
-        sk, n = self.batch.sk_get(slot, 0)
-        ck = Checkpoint(job, r, x, xo, nz, self.batch.step_count(slot), sk * n if n else None, n, epochs_run)
-        self.batch.set_active(slot, False)
+        b, i = self._b(slot)
+        x, xo, nz = b.get_state(i)
+        sk, n = b.sk_get(i, 0)
+        ck = Checkpoint(job, r, x, xo, nz, b.step_count(i), sk * n if n else None, n, epochs_run)
+        b.set_active(i, False)
         self.free[r.grid].append(slot)
         return ck
 
     def _start(self, slot: int, item, now: float):
         """Puts a new job or a checkpoint into `slot` and activates it."""
+        b, i = self._b(slot)
         if isinstance(item, Checkpoint):
             job, r = item.job, item.result
-            self.batch.load(slot, job.system, activate=False)
-            self.batch.set_state(slot, item.x, item.xo, item.noise)
-            self.batch.set_step(slot, item.step)
+            b.load(i, job.system, activate=False)
+            b.set_state(i, item.x, item.xo, item.noise)
+            b.set_step(i, item.step)
             r.slot = slot
         else:
             job = item
             r = JobResult(job.job_id, job.system.ns, grid_edge(job.system), job.steps, job.arrival, admitted=now,
                           slot=slot)
-            self.batch.load(slot, job.system, activate=False)
-        self.batch.set_stop(slot, job.steps)
-        self.batch.set_active(slot, True)
+            b.load(i, job.system, activate=False)
+        b.set_stop(i, job.steps)
+        b.set_active(i, True)
         return job, r
+
+    def _advance(self, running: dict):
+        """One epoch on every pool with a running job (concurrently), then each pool's force
+        evaluation at the new positions."""
+        busy = sorted({self.slot_at[sid][0] for sid in running})
+
+        def one(pid):
+            b = self.pools[pid].batch
+            b.step(self.epoch)
+            b.evaluate()
+
+        if len(busy) == 1:
+            one(busy[0])
+        else:
+            for f in [self._exec.submit(one, pid) for pid in busy]:
+                f.result()
+        for pid, p in self.pools.items():
+            p.idle = 0 if pid in busy else p.idle + 1
 
     def run(self, jobs: Sequence[Job], clock: str = "wall", time_slice: Optional[int] = None,
             preempt_at: Optional[Dict[int, int]] = None) -> List[JobResult]:
@@ -189,7 +325,7 @@ class Server:
         preempts.  preempt_at: {job_id: epoch} checkpoints that job once, after that many of its
         epochs (tests)."""
         for j in jobs:
-            if grid_edge(j.system) not in self.free:
+            if grid_edge(j.system) not in self.edges:
                 raise ValueError(f"job {j.job_id}: no slot has grid edge {grid_edge(j.system)}")
             if j.steps < 1:
                 raise ValueError(f"job {j.job_id}: steps must be positive")
@@ -213,8 +349,11 @@ class Server:
             while pending and pending[0].arrival <= t:
                 queue.append(pending.popleft())
             waiting = []
+            blocked = set()                   # shapes the budget cannot grow this round
             for item in queue:
                 g = edge_of(item)
+                if not self.free[g] and self.grow and g not in blocked and not self._try_grow(g, running):
+                    blocked.add(g)
                 if self.free[g]:
                     slot = self.free[g].popleft()
                     job, r = self._start(slot, item, now())
@@ -230,30 +369,33 @@ class Server:
                     epoch_no = max(epoch_no + 1, int(math.ceil(pending[0].arrival)))
                 continue
             ts0 = time.perf_counter()
-            before = {slot: self.batch.step_count(slot) for slot in running}
-            self.batch.step(self.epoch)
+            before = {}
+            for slot in running:
+                b, i = self._b(slot)
+                before[slot] = b.step_count(i)
             # records describe each job's state after the epoch (stopped jobs: their last step)
-            self.batch.evaluate()
+            self._advance(running)
             self.stepping_s += time.perf_counter() - ts0
             self.epochs_run += 1
             epoch_no += 1
             waiting_edges = collections.Counter(edge_of(it) for it in queue)
             for slot in list(running):
                 job, r, ran = running[slot]
+                b, i = self._b(slot)
                 ran += 1
                 running[slot][2] = ran
-                o = self.batch.observables(slot)
-                step_now = self.batch.step_count(slot)
+                o = b.observables(i)
+                step_now = b.step_count(i)
                 self.work_done += (step_now - before[slot]) * job.system.ns
                 r.energy.append((step_now, o["upe"]))
-                self.batch.sk_accumulate(slot, 0, job.sk_type)
-                if not self.batch.active(slot):
-                    sk, n = self.batch.sk_get(slot, 0)
+                b.sk_accumulate(i, 0, job.sk_type)
+                if not b.active(i):
+                    sk, n = b.sk_get(i, 0)
                     parts = sk_parts.pop(job.job_id, []) + [(sk * n, n)]
                     r.sk_calls = sum(k for _, k in parts)
                     r.sk = sum(v for v, _ in parts) / r.sk_calls
                     if self.keep_positions:
-                        r.x = self.batch.get_state(slot)[0]
+                        r.x = b.get_state(i)[0]
                     r.finished = now()
                     del running[slot]
                     self.free[r.grid].append(slot)
@@ -269,6 +411,12 @@ class Server:
                     del running[slot]
                     queue.append(ck)
                     waiting_edges[r.grid] -= 1
+            # grown pools with nothing to run for a while give their memory back
+            if self.grow:
+                busy = {self.slot_at[sid][0] for sid in running}
+                for p in list(self.pools.values()):
+                    if p.grown and p.pid not in busy and p.idle >= self.idle_epochs:
+                        self._release(p)
         return [results[j.job_id] for j in jobs]
 
 

@@ -3,7 +3,9 @@
 #   _ref/ref_harness   reference objects minus main.o + ref_harness_main.cu: runs
 #                      initialize(); forces(); and dumps forces, densities and stencils
 # Nothing here is product code.  Usage: make -f ref.mk REF=<path to the gpu-tild sources>
-REF      ?= /root/reference
+ifeq ($(REF),)
+$(error REF=<path to the gpu-tild sources> is required)
+endif
 NVCC     ?= nvcc
 OUT      := _ref
 FLAGS    := -std=c++14 -rdc=true -gencode arch=compute_100a,code=sm_100a -O3 -w

@@ -1,7 +1,7 @@
 """Builds the committed golden fixtures from the reference's own example files.
 
-Run in a checkout where the gpu-tild sources are available (default location below); the GPU
-box never needs them.  Outputs, next to this script:
+Usage: python make_golden.py <path to the gpu-tild sources>.  Only a checkout that has those
+sources runs it; the GPU box never needs them.  Outputs, next to this script:
   coacervate_config.npz   examples/Coacervate/input.data parsed as read_charge_config does
                           (positions FP32 via %f, types, charges, bond list)
   coacervate_step0.json   the step-0 line of examples/Coacervate/data.dat, the input script
@@ -18,10 +18,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(HERE, "..", "..", "gpu-tild_b200")]
 import tild_systems as ts  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-
-
 def main():
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python make_golden.py <path to the gpu-tild sources>")
+    REF = sys.argv[1]
     ex = os.path.join(REF, "examples", "Coacervate")
     d = ts.read_data_file(os.path.join(ex, "input.data"), 3, True)
     np.savez_compressed(os.path.join(HERE, "coacervate_config.npz"), x=d["x"], types=d["types"].astype(np.int8),

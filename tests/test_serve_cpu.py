@@ -143,3 +143,38 @@ def test_time_slice_preempts_and_resumes_from_checkpoints():
     assert [s for s, _ in by[1].energy] == [64, 128]
     assert by[1].finished == 4 and by[0].finished == 6
     assert by[0].sk_calls == 4 and by[1].sk_calls == 2
+
+
+def test_growth_admits_a_burst_beyond_the_initial_slots():
+    """Admission by memory: a burst of one grid shape larger than the initial slots of that shape
+    is admitted at once into pools grown for it, while the budget allows."""
+    srv = FakeServer({24: 1, 26: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                     measure_memory=False, grow=True, group_slots=2, hbm_budget=1e9)
+    jobs = [sv.Job(k, tiny(24, 10 + k), 128, 0) for k in range(5)]
+    res = srv.run(jobs, clock="epochs")
+    assert all(r.admitted == 0 and r.finished == 2 for r in res)
+    assert srv.pools_grown == 2 and len({r.slot for r in res}) == 5
+
+
+def test_growth_stops_at_the_hbm_budget():
+    one = sv.slot_bytes_estimate(24, 100)
+    # the two-slot initial pool plus exactly one grown pool of two slots fit
+    budget = 2 * one + 2 * one + one // 2
+    srv = FakeServer({24: 1, 26: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                     measure_memory=False, grow=True, group_slots=2, hbm_budget=budget)
+    jobs = [sv.Job(k, tiny(24, 20 + k), 64, 0) for k in range(5)]
+    res = srv.run(jobs, clock="epochs")
+    by = {r.job_id: r for r in res}
+    assert srv.pools_grown == 1 and srv.peak_bytes <= budget
+    assert [by[k].admitted for k in range(5)] == [0, 0, 0, 1, 1]      # two wait one epoch
+
+
+def test_idle_grown_pools_release_their_memory():
+    srv = FakeServer({24: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                     measure_memory=False, grow=True, group_slots=2, idle_epochs=2, hbm_budget=1e9)
+    burst = [sv.Job(k, tiny(24, 30 + k), 64, 0) for k in range(3)]
+    late = [sv.Job(3, tiny(24, 40), 64 * 6, 0)]            # keeps the loop running after the burst
+    res = srv.run(burst + late, clock="epochs")
+    assert srv.pools_grown == 2 and srv.pools_released >= 1
+    assert all(r.finished == 1 for r in res[:3]) and res[3].finished == 6
+    assert len(srv.pools) <= 2

@@ -111,3 +111,22 @@ def test_preempted_job_resumes_bitwise():
     assert np.array_equal(ra.x, whole.x)
     assert ra.sk_calls == whole.sk_calls
     assert np.allclose(ra.sk, whole.sk, rtol=1e-12, atol=1e-12 * np.abs(whole.sk).max())
+
+
+def test_burst_of_one_shape_admitted_by_memory():
+    """With pools grown inside the HBM budget, a burst of 14 jobs of one grid shape (2 initial
+    slots) is admitted at once; each job's trace matches the same job served alone."""
+    jobs = [sv.Job(k, job_system(24, 50 + k, N=10 + (k % 3) * 4), 128 + 64 * (k % 2), 0) for k in range(14)]
+    with sv.Server({24: 2, 26: 1}, epoch=64, keep_positions=True, grow=True, group_slots=4) as srv:
+        res = srv.run(jobs, clock="epochs")
+        grown, peak = srv.pools_grown, srv.peak_bytes
+    assert grown == 3 and peak <= 80e9
+    assert all(r.admitted == 0 for r in res)
+    for k in (0, 5, 13):
+        with sv.Server({24: 1}, epoch=64, keep_positions=True, measure_memory=False) as alone_srv:
+            ra = alone_srv.run([sv.Job(k, jobs[k].system, jobs[k].steps, 0)], clock="epochs")[0]
+        em = np.array([e for _, e in res[k].energy])
+        ea = np.array([e for _, e in ra.energy])
+        assert [s for s, _ in res[k].energy] == [s for s, _ in ra.energy]
+        assert np.max(np.abs(em - ea) / np.abs(ea)) < ENERGY_RTOL
+        assert min_image_maxdiff(res[k].x, ra.x, jobs[k].system.box) < POS_ATOL
