@@ -130,7 +130,7 @@ def ensemble_leg(grp, args) -> dict:
             ref_sample = sample[::4]
             t_ref, ns_ref = 0.0, 0
             for i in ref_sample:
-                r = reference_cuda(systems[i], "ensemble_member", pairs=1)
+                r = reference_cuda(systems[i], "ensemble_member", runs=1, target_s=0.5)
                 if r is None or "unavailable" in r:
                     t_ref = None
                     break
@@ -394,7 +394,10 @@ def run_ours(args):
     x_in = tild.HostArray((s.ns, s.dim))   # page-locked host buffers, filled/allocated before timing
     x_in.array[:] = s.x
     x_out = tild.HostArray((s.ns, s.dim))
-    ctx.observables()   # untimed: the first call allocates the reduction scratch once
+    # untimed: the first observables call allocates the reduction scratch and the first snapshot
+    # its device buffers and copy stream, once per context
+    ctx.observables()
+    ctx.snapshot_wait(ctx.snapshot_async(x_out.array, None))
     ctx.sync()
     t0 = time.perf_counter()
     ctx.set_state(x_in.array)
@@ -473,38 +476,38 @@ def cpu_baseline(s, args, target_s: float = 20.0):
                       f"(oracle/tild_oracle.c, FP64, OpenMP {cores} threads)"}
 
 
-def reference_cuda(s, wname, steps=None, pairs: int = 3):
-    """The reference program built from its own sources (oracle/_ref/gpu-tild) on this GPU:
-    per-step time = difference of wall times of two runs that differ only in max_steps, so setup
-    and output cancel.  The longer run is sized (about 3 s of stepping at the reference's rate
-    per bead, at least 100 steps) so the difference dominates the spread of process start-up;
-    `pairs` such pairs are timed and the median is reported with the range."""
-    if steps is None:
-        extra = int(min(20000, max(100, 3.0 / (s.ns * 4e-9))))
-        steps = (20, 20 + extra)
-    exe = os.path.join(ROOT, "oracle", "_ref", "gpu-tild")
+def reference_cuda(s, wname, runs: int = 3, target_s: float = 2.0):
+    """The reference's own CUDA build on this GPU: oracle/_ref/ref_harness (the unmodified reference
+    objects with a main that runs the reference's step loop, forces(); Integrate_2();
+    update_pairstyles(), output off, main.cu:104-201) times N steps with the device synchronised
+    on both sides after 10 untimed steps.  N is sized to about target_s seconds at a first
+    estimate; `runs` runs of the program, median reported with every run's value."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if not os.path.exists(exe):
         return None
     per = []
     with tempfile.TemporaryDirectory() as td:
         ts.write_data_file(os.path.join(td, "input.data"), s)
-        for _ in range(pairs):
-            times = []
-            for n in steps:
-                ts.write_input_script(os.path.join(td, "input"), s, max_steps=n, log_freq=10 ** 8, binary_freq=0)
-                t0 = time.perf_counter()
-                r = subprocess.run([exe, "-in", "input"], cwd=td, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
-                                   timeout=900)
-                times.append(time.perf_counter() - t0)
-                if r.returncode != 0:
-                    return {"unavailable": f"reference build exited {r.returncode}"}
-            per.append((times[1] - times[0]) / (steps[1] - steps[0]))
-    per_step = float(np.median(per))
+        ts.write_input_script(os.path.join(td, "input"), s, max_steps=10 ** 6, log_freq=10 ** 8, binary_freq=0)
+        n = 20
+        for k in range(runs + 1):   # the first run sizes N
+            r = subprocess.run([exe, "-in", "input", "-out", "t", "-steps", str(n), "-time", "10"], cwd=td,
+                               stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, timeout=900)
+            line = [l for l in r.stdout.splitlines() if l.startswith("harness timing:")]
+            if r.returncode != 0 or not line:
+                return {"unavailable": f"reference harness exited {r.returncode}"}
+            ms = float(line[0].split()[4])
+            if k == 0:
+                n = int(min(20000, max(50, target_s * 1e3 / max(ms, 1e-3))))
+            else:
+                per.append(ms)
+    per_step = float(np.median(per)) / 1e3
     return {"value": s.ns / per_step, "unit": "particle-steps/s", "ms_per_step": per_step * 1e3,
-            "ms_per_step_pairs": [p * 1e3 for p in per],
-            "binary": "oracle/_ref/gpu-tild (unmodified reference sources, nvcc -arch=sm_100a -O3)",
-            "method": f"median over {pairs} pairs of the wall-time difference of {steps[1]}- and {steps[0]}-step runs "
-                      "(setup and output cancel)"}
+            "ms_per_step_runs": per, "steps_timed": n,
+            "binary": "oracle/_ref/ref_harness (unmodified reference objects, nvcc -arch=sm_100a -O3, and a main "
+                      "that times the reference's step loop)",
+            "method": f"median over {runs} runs of {n} timed steps after 10 untimed ones, device synchronised on both "
+                      "sides"}
 
 
 def run_reference(args):

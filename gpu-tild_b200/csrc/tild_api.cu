@@ -36,6 +36,14 @@ __global__ void k_fill_padding(float4* __restrict__ p0, float4* __restrict__ p1,
   p1[s] = pad;
 }
 
+// flag[0] |= 1 when any of the n uploaded values is not finite
+__global__ void k_check_finite(const float* __restrict__ v, long long n, int* __restrict__ flag) {
+  bool bad = false;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(v[k]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
 __global__ void k_pack_noise(const float* __restrict__ src, const int* __restrict__ slot_of, int ns, int D,
                              float* __restrict__ noise) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -483,7 +491,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   rc = rc ? rc : dalloc(c, &c->kd, (size_t)kd, "k vectors");
   rc = rc ? rc : dalloc(c, &c->kk, (size_t)kd, "k vectors");
   rc = rc ? rc : dalloc(c, &c->xfer, (size_t)maxns * 3, "transfer buffer");
-  rc = rc ? rc : dalloc(c, &c->d_status, 1, "status");
+  rc = rc ? rc : dalloc(c, &c->d_status, 2, "status");  // [0] status word, [1] input check flag
   rc = rc ? rc : dalloc(c, &c->d_sys, (size_t)nsys, "system descriptors");
   rc = rc ? rc : dalloc(c, &c->cta_bead, tb.size(), "lookup");
   rc = rc ? rc : dalloc(c, &c->cta_spec, tspec.size(), "lookup");
@@ -491,7 +499,7 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   if (c->rng == TILD_RNG_XORWOW) rc = rc ? rc : dalloc(c, &c->xorwow, NS, "xorwow states");
   if (rc) return rc;
   cudaStream_t st = c->stream;
-  cudaMemsetAsync(c->d_status, 0, sizeof(int), st);
+  cudaMemsetAsync(c->d_status, 0, 2 * sizeof(int), st);
   cudaMemsetAsync(c->rho_fx, 0, sizeof(unsigned long long) * grid, st);
   cudaMemsetAsync(c->noise, 0, sizeof(float) * NS * 3, st);
   cudaMemsetAsync(c->bond_nbr, 0, sizeof(int) * NS * 3, st);
@@ -601,14 +609,24 @@ int sys_set_state(tild_ctx* c, int s, const float* x, const float* xo, const flo
   if (!h.topo_set) return set_err(c, TILD_ERR_STATE, "tild_set_topology must come before tild_set_state");
   cudaSetDevice(c->device);
   const size_t n = (size_t)h.ns * h.D;
-  for (size_t i = 0; i < n; i++)
-    if (!std::isfinite(x[i])) return set_err(c, TILD_ERR_NAN, "non-finite position in tild_set_state");
-  if (tild_drop_ahead(c)) return TILD_ERR_CUDA;
   const unsigned nb = nblk(h.ns, 256);
   cudaStream_t st = c->stream;
   const int* so = c->slot_of + h.bead0;
   const int* ty = c->types_dev + h.bead0;
   if (tild_check(c, cudaMemcpyAsync(c->xfer, x, n * 4, cudaMemcpyHostToDevice, st), "upload x")) return TILD_ERR_CUDA;
+  // the positions are checked on the device before anything of the current state changes
+  {
+    int bad = 0;
+    if (tild_check(c, cudaMemsetAsync(c->d_status + 1, 0, sizeof(int), st), "clear check flag")) return TILD_ERR_CUDA;
+    k_check_finite<<<std::min<unsigned>(nblk((long long)n, 256), 1184), 256, 0, st>>>(c->xfer, (long long)n,
+                                                                                        c->d_status + 1);
+    c->launches++;
+    if (tild_check(c, cudaMemcpyAsync(&bad, c->d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st), "check flag") ||
+        tild_check(c, cudaStreamSynchronize(st), "sync check"))
+      return TILD_ERR_CUDA;
+    if (bad) return set_err(c, TILD_ERR_NAN, "non-finite position in tild_set_state");
+  }
+  if (tild_drop_ahead(c)) return TILD_ERR_CUDA;
   k_pack_pos<<<nb, 256, 0, st>>>(c->xfer, ty, so, h.ns, h.D, c->pos[c->cur]);
   // x_{n-1}: xo when given, else x (send_3n_to_device copies x into xo, device_comm_utils.cu:15-16)
   if (xo && tild_check(c, cudaMemcpyAsync(c->xfer, xo, n * 4, cudaMemcpyHostToDevice, st), "upload xo"))

@@ -13,12 +13,17 @@
 //   <out>_neigh.bin d_neigh_inds int [ns][CELL_MAX]; <out>_nlist.txt CELL_MAX total_ncells
 //   (the caller checks on the host first that no cell or row overflows CELL_MAX: the reference
 //   kernels do not bound their writes)
-// Options: -in <script> -out <prefix> [-steps N] [-nonoise] [-ninds K] [-nlist rc group]
+// Options: -in <script> -out <prefix> [-steps N] [-nonoise] [-ninds K] [-nlist rc group] [-time W]
 //   -ninds K dumps the stencils of the first K beads only (large systems)
+//   -time W: timing only (no dumps): W untimed steps, then N steps of the reference's main loop
+//   with output off (Integrate_1 is a no-op for GJF/EM and check_cudaError only reads the error
+//   state, main.cu:104-201), timed with the device synchronised on both sides; prints
+//   "harness timing: <N> steps <ms> ms per step"
 // Test infrastructure only (it links the reference build); nothing in the product uses it.
 #define MAIN
 #include "globals.h"
 #include "timing.h"
+#include <chrono>
 #include <cstdio>
 #include <string>
 
@@ -54,6 +59,7 @@ int main(int argc, char** argv) {
   float nl_rc = 0.0f;
   int nsteps = 0, nonoise = 0;
   long long ninds = -1;
+  int time_warm = -1;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     if (a == "-in" && i + 1 < argc) input_file = argv[++i];
@@ -61,6 +67,7 @@ int main(int argc, char** argv) {
     else if (a == "-steps" && i + 1 < argc) nsteps = atoi(argv[++i]);
     else if (a == "-nonoise") nonoise = 1;
     else if (a == "-ninds" && i + 1 < argc) ninds = atoll(argv[++i]);
+    else if (a == "-time" && i + 1 < argc) time_warm = atoi(argv[++i]);
     else if (a == "-nlist" && i + 2 < argc) {
       nl_rc = (float)atof(argv[++i]);
       nl_group = argv[++i];
@@ -69,6 +76,29 @@ int main(int argc, char** argv) {
   initialize();
   if (nonoise) noise_mag = 0.0f;
   step = 0;
+  if (time_warm >= 0) {
+    for (step = 1; step <= time_warm; step++) {
+      forces();
+      for (int i = 0; i < n_integrators; i++) Integrators[i].Integrate_2();
+      update_pairstyles();
+    }
+    cudaDeviceSynchronize();
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < nsteps; k++, step++) {
+      forces();
+      for (int i = 0; i < n_integrators; i++) Integrators[i].Integrate_2();
+      update_pairstyles();
+    }
+    cudaDeviceSynchronize();
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      fprintf(stderr, "harness: CUDA error %s\n", cudaGetErrorString(e));
+      return 1;
+    }
+    printf("harness timing: %d steps %.6f ms per step\n", nsteps, nsteps > 0 ? ms / nsteps : 0.0);
+    return 0;
+  }
   dump(out + "_x0.bin", d_x, sizeof(float) * ns * Dim);
   if (!nl_group.empty()) {
     NList nl;
