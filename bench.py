@@ -294,10 +294,13 @@ def step_bytes(s) -> int:
     return s.ns * bp + M * 48 * (s.ntypes + C)
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the stage's kernel, from one ncu
-# capture of that kernel on the same workload (summaries and commands under profiles/)
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the stage's kernel on this
+# workload: one ncu capture of k_gather<3,3,GJF> and k_spread_tiled<3,3> on the half-size blend
+# (--workload blend_half, one launch each inside the timed region, counters dram__bytes_read.sum
+# and dram__bytes_write.sum), doubled: the full blend has twice the beads and twice the grid
+# points, and both kernels' traffic grows in proportion.
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 298451456, "spread": 75735808},
+    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 2 * (125391872 + 17887232), "spread": 2 * 37661440},
 }
 
 
