@@ -680,7 +680,7 @@ bool all_ready(tild_ctx* c) {
 
 // Host bookkeeping of `n` integrating steps that ran inside a graph replay (the device side,
 // including step counters and buffer rotations, is in the graph).
-void account_replayed_steps(tild_ctx* c, int n, long long launches_per_step) {
+void account_replayed_steps(tild_ctx* c, int n, long long launches, int nsorts) {
   for (int s = 0; s < c->nsys; s++) {
     SysHost& h = c->sys[s];
     if (!h.active) continue;
@@ -689,81 +689,97 @@ void account_replayed_steps(tild_ctx* c, int n, long long launches_per_step) {
     h.forces_step = h.step;
     h.have_forces = true;
   }
-  c->launches += launches_per_step * n;
-  if (c->sort_interval > 0) c->sorts += n / c->sort_interval;
+  c->launches += launches;
+  c->sorts += nsorts;
 }
 
-// n integrating steps.  Whole periods of graph_len steps (two sort periods, so every buffer
-// rotation and sort swap returns to its starting configuration) run as one CUDA graph, captured
-// once per buffer configuration and replayed afterwards; the rest run as direct launches.
+constexpr int kMinGraphSteps = 8;  // shorter runs launch directly
+
+// n integrating steps as CUDA graphs.  Whole periods of graph_len steps (two sort periods, so
+// every buffer rotation and sort trade returns to its starting configuration) start with a sort;
+// a remainder of at least kMinGraphSteps steps (or a run that starts between sorts) is a graph
+// of its own length.  A graph is captured once per starting configuration (buffers, rotation,
+// sort phase, spread-ahead state, transformed grid shapes, length) and replayed afterwards; a
+// replay moves the host mirrors to the configuration the capture ended in.  Shorter remainders
+// run as direct launches.
 int run_steps(tild_ctx* c, int n) {
   const int len = c->sort_interval > 0 ? 2 * c->sort_interval : c->graph_len;
   while (n > 0) {
     const bool aligned = c->sort_interval <= 0 || c->steps_since_sort >= c->sort_interval;
-    if (c->use_graphs && n >= len && aligned && !c->profiling) {
-      c->steps_since_sort = c->sort_interval;  // the graph always starts with a sort
-      const void* p0 = c->pos[0];
-      const int cur = c->cur;
-      const std::vector<char> on = tild_buckets_on(c);
-      const bool ahead = c->rho_ahead;  // whether the period's first step spreads
-      cudaGraphExec_t exec = nullptr;
-      bool ahead_end = false;
-      for (auto& ge : c->graphs)
-        if (ge.p0 == p0 && ge.cur == cur && ge.buckets_on == on && ge.ahead == ahead) {
-          exec = ge.exec;
-          ahead_end = ge.ahead_end;
-        }
-      if (!exec) {
-        const long long l0 = c->launches;
-        const int64_t step_before = c->sys[0].step;
-        std::vector<SysHost> saved_hosts;  // host counters advance during capture; restore, then replay
-        for (const SysHost& h : c->sys) saved_hosts.push_back(h);
-        const auto saved_hsys = c->h_sys;
-        const long long saved_sorts = c->sorts;
-        if (tild_check(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture"))
-          return TILD_ERR_CUDA;
-        int rc = TILD_OK;
-        for (int k = 0; k < len && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
-        cudaGraph_t graph = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
-        if (rc) {
-          if (graph) cudaGraphDestroy(graph);
-          return rc;
-        }
-        if (tild_check(c, e, "end capture")) return TILD_ERR_CUDA;
-        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (tild_check(c, ei, "instantiate graph")) return TILD_ERR_CUDA;
-        (void)step_before;
-        // capture advanced the host mirrors without running anything: restore them
-        const long long per_step = (c->launches - l0) / len;
-        for (int s = 0; s < c->nsys; s++) {
-          c->sys[s].step = saved_hosts[s].step;
-          c->sys[s].forces_step = saved_hosts[s].forces_step;
-          c->sys[s].have_forces = saved_hosts[s].have_forces;
-        }
-        c->h_sys = saved_hsys;
-        c->sorts = saved_sorts;
-        c->launches = l0;
-        if (c->graphs.size() >= 8) {  // keep the eight most recent configurations
-          cudaGraphExecDestroy(c->graphs.front().exec);
-          c->graphs.erase(c->graphs.begin());
-        }
-        ahead_end = c->rho_ahead;
-        c->graphs.push_back({exec, p0, cur, on, ahead, ahead_end});
-        c->graph_launches_per_step = per_step;
-        // after capture the buffer configuration is back at (p0, cur): same as a replay
-      }
-      if (tild_check(c, cudaGraphLaunch(exec, c->stream), "graph launch")) return TILD_ERR_CUDA;
-      c->rho_ahead = ahead_end;
-      account_replayed_steps(c, len, c->graph_launches_per_step);
-      c->steps_since_sort = c->sort_interval;
-      n -= len;
-    } else {
+    int L = 0;
+    if (c->use_graphs && !c->profiling) {
+      if (n >= len && aligned) L = len;
+      else if (n >= kMinGraphSteps) L = std::min(n, len);
+    }
+    if (L == 0) {
       int rc = tild_run_forces(c, true, nullptr, -1);
       if (rc) return rc;
       n -= 1;
+      continue;
     }
+    if (L == len && aligned) c->steps_since_sort = c->sort_interval;  // a whole period starts with a sort
+    const void* p0 = c->pos[0];
+    const int cur = c->cur;
+    const int64_t sss0 = c->steps_since_sort;
+    const std::vector<char> on = tild_buckets_on(c);
+    const bool ahead = c->rho_ahead;  // whether the graph's first step spreads
+    const tild_ctx::GraphEntry* found = nullptr;
+    for (const auto& ge : c->graphs)
+      if (ge.p0 == p0 && ge.cur == cur && ge.buckets_on == on && ge.ahead == ahead && ge.len == L && ge.sss0 == sss0)
+        found = &ge;
+    if (found) {
+      const tild_ctx::GraphEntry ge = *found;
+      if (tild_check(c, cudaGraphLaunch(ge.exec, c->stream), "graph launch")) return TILD_ERR_CUDA;
+      c->cur = ge.cur_end;
+      for (int k = 0; k < (ge.nsorts & 1); k++) tild_sort_swap_buffers(c);
+      c->steps_since_sort = ge.sss_end;
+      c->rho_ahead = ge.ahead_end;
+      account_replayed_steps(c, L, ge.launches, ge.nsorts);
+      n -= L;
+      continue;
+    }
+    // capture: the host code runs the steps' launches into the graph and leaves every host
+    // mirror of the buffers at the configuration after them; the step counters are put back
+    // and advance when the graph runs
+    const long long l0 = c->launches;
+    std::vector<SysHost> saved_hosts;
+    for (const SysHost& h : c->sys) saved_hosts.push_back(h);
+    const auto saved_hsys = c->h_sys;
+    const long long saved_sorts = c->sorts;
+    if (tild_check(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "begin capture"))
+      return TILD_ERR_CUDA;
+    int rc = TILD_OK;
+    for (int k = 0; k < L && !rc; k++) rc = tild_run_forces(c, true, nullptr, -1);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (tild_check(c, e, "end capture")) return TILD_ERR_CUDA;
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (tild_check(c, ei, "instantiate graph")) return TILD_ERR_CUDA;
+    const long long glaunches = c->launches - l0;
+    const int nsorts = (int)(c->sorts - saved_sorts);
+    for (int s = 0; s < c->nsys; s++) {
+      c->sys[s].step = saved_hosts[s].step;
+      c->sys[s].forces_step = saved_hosts[s].forces_step;
+      c->sys[s].have_forces = saved_hosts[s].have_forces;
+    }
+    c->h_sys = saved_hsys;
+    c->sorts = saved_sorts;
+    c->launches = l0;
+    if (c->graphs.size() >= 8) {  // keep the eight most recent configurations
+      cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back({exec, p0, cur, on, ahead, c->rho_ahead, L, sss0, c->steps_since_sort, c->cur, nsorts, glaunches});
+    c->graph_launches_per_step = glaunches / L;
+    if (tild_check(c, cudaGraphLaunch(exec, c->stream), "graph launch")) return TILD_ERR_CUDA;
+    account_replayed_steps(c, L, glaunches, nsorts);
+    n -= L;
   }
   return TILD_OK;
 }

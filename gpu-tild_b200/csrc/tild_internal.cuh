@@ -215,7 +215,12 @@ struct tild_ctx {
     const void* p0;
     int cur;
     std::vector<char> buckets_on;        // grid shapes whose transforms the graph runs
-    bool ahead, ahead_end;               // rho_ahead before and after the period
+    bool ahead, ahead_end;               // rho_ahead before and after the graph's steps
+    int len;                             // steps in the graph
+    int64_t sss0, sss_end;               // steps_since_sort before and after
+    int cur_end;                         // buffer rotation after
+    int nsorts;                          // sorts inside (each trades every per-slot array once)
+    long long launches;                  // libtild kernel launches inside
   };
   std::vector<GraphEntry> graphs;
   bool use_graphs = true;
@@ -459,4 +464,5 @@ int tild_ensure_red(tild_ctx* c, int nvals, int nblocks);
 int tild_sort_alloc(tild_ctx* c);                     // tild_sort.cu
 void tild_sort_free(tild_ctx* c);
 int tild_sort_beads(tild_ctx* c);
+void tild_sort_swap_buffers(tild_ctx* c);
 int tild_upload_sys(tild_ctx* c);                     // tild_api.cu: copies h_sys to d_sys

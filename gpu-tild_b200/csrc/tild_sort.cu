@@ -163,6 +163,19 @@ void tild_sort_free(tild_ctx* c) {
     if (p) cudaFree(p);
 }
 
+// The permuted arrays become the current ones: every per-slot array trades places with its
+// alternate.  A replayed CUDA graph that contains sorts applies the same trades on the host.
+void tild_sort_swap_buffers(tild_ctx* c) {
+  std::swap(c->pos[0], c->alt_pos[0]);
+  std::swap(c->pos[1], c->alt_pos[1]);
+  std::swap(c->noise, c->alt_noise);
+  std::swap(c->bead_id, c->alt_bead_id);
+  std::swap(c->bond_info, c->alt_info);
+  std::swap(c->bond_nbr, c->alt_nbr);
+  if (c->charge) std::swap(c->charge, c->alt_charge);
+  if (c->xorwow) std::swap(c->xorwow, c->alt_xorwow);
+}
+
 int tild_sort_beads(tild_ctx* c) {
   if (!c->sort_temp) return TILD_OK;
   const int n = c->nslots;
@@ -185,14 +198,7 @@ int tild_sort_beads(tild_ctx* c) {
   k_remap_bonds<<<nb, kTile, 0, st>>>(c->sort_perm, n, c->bond_nbr, c->alt_info, c->sort_newslot, c->alt_bead_id,
                                       c->cta_bead, c->d_sys, c->alt_nbr, c->slot_of);
   c->launches += 2;
-  std::swap(c->pos[0], c->alt_pos[0]);
-  std::swap(c->pos[1], c->alt_pos[1]);
-  std::swap(c->noise, c->alt_noise);
-  std::swap(c->bead_id, c->alt_bead_id);
-  std::swap(c->bond_info, c->alt_info);
-  std::swap(c->bond_nbr, c->alt_nbr);
-  if (c->charge) std::swap(c->charge, c->alt_charge);
-  if (c->xorwow) std::swap(c->xorwow, c->alt_xorwow);
+  tild_sort_swap_buffers(c);
   c->steps_since_sort = 0;
   c->sorts++;
   return tild_check(c, cudaGetLastError(), "sort") ? TILD_ERR_CUDA : TILD_OK;

@@ -102,6 +102,40 @@ def test_graph_replay_matches_direct_steps():
     np.testing.assert_array_equal(ng, nd)
 
 
+@pytest.mark.parametrize("pmeorder,chunks", [(1, [20] * 5), (1, [9, 45, 13, 8, 25]), (3, [20] * 5),
+                                              (3, [31, 17, 10, 40])])
+def test_graphs_of_any_length_match_direct_steps(pmeorder, chunks):
+    """Runs shorter than a whole period, or starting between sorts, replay graphs of their own
+    length (captured per starting configuration): bit-identical to one step per call, whatever
+    the split, and the replays leave the host at the right buffers and sort phase."""
+    s = small_diblock(3, pmeorder, nx=(16, 18, 20), box=(8.0, 9.0, 10.0))
+    n = sum(chunks)
+    with tild.Context(s) as c:
+        for k in chunks:
+            c.step(k)
+        for k in chunks:                 # the same split again: every graph is replayed
+            c.step(k)
+        xg, xog, ng = c.get_state()
+        assert c.step_count == 2 * n
+    with tild.Context(s) as c:
+        for _ in range(2 * n):
+            c.step(1)
+        xd, xod, nd = c.get_state()
+    np.testing.assert_array_equal(xg, xd)
+    np.testing.assert_array_equal(xog, xod)
+    np.testing.assert_array_equal(ng, nd)
+
+
+def test_batch_stops_inside_a_remainder_graph():
+    systems = mixed_systems()[:3]
+    with tild.Batch(systems) as B:
+        B.set_stop(1, 13)
+        B.step(20)                       # one graph of 20 steps; system 1 stops after its 13th
+        assert [B.step_count(i) for i in range(3)] == [20, 13, 20] and not B.active(1)
+        B.step(20)
+        assert [B.step_count(i) for i in range(3)] == [40, 13, 40]
+
+
 def test_batch_graph_with_inactive_system():
     systems = mixed_systems()[:3]
     with tild.Batch(systems) as B:
