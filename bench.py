@@ -183,8 +183,9 @@ def run_ensemble(args):
 def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True) -> dict:
     """Serving: a seeded Poisson stream (mean `rate` jobs/s) of `njobs` jobs drawn from the
     batched-ensemble distribution, each --job-steps steps returning its energy trace and avg_sk,
-    served by continuous batching over slot pools (--slots-per-edge initial slots for each grid
-    edge 24..48, more grown on demand inside the HBM budget).  value: aggregate particle-steps/s
+    served by continuous batching over slot pools grown on demand inside the HBM budget (one slot
+    per queued job of a grid shape, up to --group-slots per pool; --slots-per-edge initial slots
+    for each grid edge 24..48, none by default).  value: aggregate particle-steps/s
     of all jobs over the span from the first arrival to the last completion; latency percentiles
     are arrival -> results on the host.  Against: the same jobs run one at a time alone (a sample
     of them, each for all its steps, set-up included)."""
@@ -557,8 +558,10 @@ def main():
     ap.add_argument("--jobs", type=int, default=300, help="serving: number of jobs in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: mean arrivals per second")
     ap.add_argument("--job-steps", type=int, default=5000)
-    ap.add_argument("--slots-per-edge", type=int, default=12, help="serving: initial slots per grid edge")
-    ap.add_argument("--group-slots", type=int, default=8, help="serving: slots of a pool grown on demand")
+    ap.add_argument("--slots-per-edge", type=int, default=0,
+                    help="serving: initial slots per grid edge (0: every slot grown on demand)")
+    ap.add_argument("--group-slots", type=int, default=8,
+                    help="serving: largest pool grown on demand (one slot per queued job of the shape)")
     ap.add_argument("--no-grow", action="store_true", help="serving: fixed slots only")
     ap.add_argument("--subsat-rate", type=float, default=4.0, help="serving: the below-capacity arrival rate")
     ap.add_argument("--subsat-jobs", type=int, default=40)

@@ -133,6 +133,8 @@ class Server:
     epoch: steps per stepping call (a multiple of 32 keeps every call inside CUDA graphs).
     grow: create a pool of `group_slots` slots for a grid shape whose slots are all busy while a
       job of that shape waits and the budget allows; release grown pools idle for `idle_epochs`.
+      With grow, slots_per_edge may be empty: every slot is then grown on demand.
+    workers: threads that step the pools of one epoch concurrently.
     Slots are named by integers that stay unique for the server's lifetime.
     """
 
@@ -140,7 +142,7 @@ class Server:
                  template_of: Callable[[int], tild.System] = ts.ensemble_slot_template, device: int = 0,
                  hbm_budget: float = 80e9, epoch: int = 128, keep_positions: bool = False,
                  measure_memory: bool = True, tune: bool = False, grow: bool = False, group_slots: int = 4,
-                 idle_epochs: int = 2):
+                 idle_epochs: int = 2, workers: int = 16):
         self.device = device
         self.epoch = int(epoch)
         self.keep_positions = keep_positions
@@ -161,20 +163,25 @@ class Server:
         self.pools_released = 0
         self.peak_bytes = 0
         edges = [g for g, n in sorted(slots_per_edge.items()) for _ in range(n)]
-        pool = self._new_pool(edges, grown=False)
-        if pool.nbytes > self.hbm_budget:
-            pool.batch.close()
-            raise MemoryError(f"slot pool needs {pool.nbytes / 1e9:.1f} GB, budget {self.hbm_budget / 1e9:.1f} GB")
-        # schedule chosen on the initial pool (every slot holding its template system); grown
-        # pools take it too, with their single grid shape's FFTs on the main stream
-        self.schedule = pool.batch.autotune(trial_steps=64) if tune else None
-        self._tune = pool.batch.get_tune() if tune else None
-        self._register(pool)
+        if not edges and not grow:
+            raise ValueError("no initial slots and no growth: nothing could run")
+        self.schedule, self._tune = None, None
+        if edges:
+            pool = self._new_pool(edges, grown=False)
+            if pool.nbytes > self.hbm_budget:
+                pool.batch.close()
+                raise MemoryError(f"slot pool needs {pool.nbytes / 1e9:.1f} GB, budget {self.hbm_budget / 1e9:.1f} GB")
+            # schedule chosen on the initial pool (every slot holding its template system); grown
+            # pools take it too, with their single grid shape's FFTs on the main stream
+            if tune:
+                self.schedule = pool.batch.autotune(trial_steps=64)
+                self._tune = pool.batch.get_tune()
+            self._register(pool)
         self.nslots = len(edges)
         self.epochs_run = 0
         self.stepping_s = 0.0     # wall time of the stepping calls and their force evaluation
         self.work_done = 0        # particle-steps the jobs advanced inside those calls
-        self._exec = concurrent.futures.ThreadPoolExecutor(max_workers=8)
+        self._exec = concurrent.futures.ThreadPoolExecutor(max_workers=workers)
 
     @property
     def pool_bytes(self) -> int:
@@ -221,12 +228,14 @@ class Server:
         pool.batch.close()
         self.pools_released += 1
 
-    def _try_grow(self, g: int, running: dict) -> bool:
-        """A pool of group_slots slots of edge g, if the budget allows (idle grown pools of other
-        shapes are released first when that makes room).  Returns whether slots were added."""
-        caps = [max(self.capacity_of(g), self.template_of(g).ns)] * self.group_slots
+    def _try_grow(self, g: int, running: dict, demand: int = 0) -> bool:
+        """A pool of edge g with one slot per queued job of that shape (demand), at most
+        group_slots, if the budget allows (idle grown pools of other shapes are released first
+        when that makes room).  Returns whether slots were added."""
+        n = max(1, min(self.group_slots, demand or self.group_slots))
+        caps = [max(self.capacity_of(g), self.template_of(g).ns)] * n
         need = sum(slot_bytes_estimate(g, c) for c in caps)
-        known = [p for p in self.pools.values() if p.grown and p.edges[0] == g]
+        known = [p for p in self.pools.values() if p.grown and p.edges[0] == g and len(p.edges) == n]
         if known:
             need = known[0].nbytes
         if self.pool_bytes + need > self.hbm_budget:
@@ -236,7 +245,7 @@ class Server:
                     self._release(p)
             if self.pool_bytes + need > self.hbm_budget:
                 return False
-        pool = self._new_pool([g] * self.group_slots, grown=True)
+        pool = self._new_pool([g] * n, grown=True)
         if self._tune is not None:
             t = pool.batch.get_tune()
             for f, _ in tild.Tune._fields_:
@@ -350,10 +359,12 @@ class Server:
                 queue.append(pending.popleft())
             waiting = []
             blocked = set()                   # shapes the budget cannot grow this round
+            demand = collections.Counter(edge_of(it) for it in queue)
             for item in queue:
                 g = edge_of(item)
-                if not self.free[g] and self.grow and g not in blocked and not self._try_grow(g, running):
+                if not self.free[g] and self.grow and g not in blocked and not self._try_grow(g, running, demand[g]):
                     blocked.add(g)
+                demand[g] -= 1
                 if self.free[g]:
                     slot = self.free[g].popleft()
                     job, r = self._start(slot, item, now())
