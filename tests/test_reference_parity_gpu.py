@@ -222,3 +222,38 @@ def test_neighbour_list_matches_reference_build(tmp_path, rc, group):
         assert sorted(ref["neigh"][i, :n].tolist()) == gnb[i, :n].tolist()
     print(f"nlist rc={rc} group={gname}: {int(sel.sum())} beads, CELL_MAX {gcm}, "
           f"{int(gn[sel].sum())} neighbour entries equal as sets")
+
+
+# ---------------------------------------------------------------------------------------------
+# Beads on the faces of the box: x = 0 and x = L are both legal positions for the reference (its
+# integrators wrap only x > L and x < 0, device_GJF_integrator.cu:52-55), and their stencils wrap
+# across the periodic boundary (device_grid_utils.cu:305-325)
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("pmeorder", [1, 2, 3, 4])
+def test_beads_on_the_box_faces(tmp_path, pmeorder):
+    s = small_diblock(3, pmeorder)
+    L = np.array(s.box[:3], np.float32)
+    x = s.x.copy()
+    x[0] = [0.0, 0.0, 0.0]
+    x[1] = L
+    x[2] = [L[0], 0.0, L[2] * 0.5]
+    x[3] = [0.0, L[1], 0.0]
+    x[4] = [L[0] * 0.25, L[1], 0.0]
+    x[5] = (L - np.float32(1e-6)).astype(np.float32)     # just below the faces (6 decimals in the file)
+    s.x = x.astype(np.float32)
+    ref = harness(tmp_path, ref_fp32(s))
+    assert np.array_equal(ref["x0"][:6], s.x[:6])      # the face beads reach the reference unrounded
+    s.x = ref["x0"]                                     # the others as the data file rounded them
+    with tild.Context(s) as c:
+        f = c.forces()
+        inds, _ = c.stencil()
+        rho = c.density()
+    assert np.array_equal(inds, ref["inds"])
+    assert rel_l2(rho[:s.ntypes], ref["rho0"]) < RHO_RTOL
+    e_ref = rel_l2(f, ref["f0"])
+    s.table_mode = tild.TABLES_FP64
+    fo = oracle.Oracle(s).forces(s.x, 0)
+    with tild.Context(s) as c:
+        e_or = rel_l2(c.forces(), fo)
+    print(f"faces p{pmeorder}: force error vs reference build {e_ref:.2e}, vs oracle {e_or:.2e}")
+    assert e_ref < FORCE_RTOL and e_or < FORCE_RTOL
