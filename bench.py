@@ -180,12 +180,13 @@ def run_ensemble(args):
         print(json.dumps(out))
 
 
-def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True) -> dict:
+def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True, slots_per_edge: int = None) -> dict:
     """Serving: a seeded Poisson stream (mean `rate` jobs/s) of `njobs` jobs drawn from the
     batched-ensemble distribution, each --job-steps steps returning its energy trace and avg_sk,
-    served by continuous batching over slot pools grown on demand inside the HBM budget (one slot
-    per queued job of a grid shape, up to --group-slots per pool; --slots-per-edge initial slots
-    for each grid edge 24..48, none by default).  value: aggregate particle-steps/s
+    served by continuous batching over slot pools: --slots-per-edge initial slots for each grid
+    edge 24..48 (12 for the 50 jobs/s stream, none for the stream below capacity) and pools grown
+    on demand inside the HBM budget (one slot per queued job of a grid shape, up to
+    --group-slots per pool).  value: aggregate particle-steps/s
     of all jobs over the span from the first arrival to the last completion; latency percentiles
     are arrival -> results on the host.  Against: the same jobs run one at a time alone (a sample
     of them, each for all its steps, set-up included)."""
@@ -193,9 +194,11 @@ def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True) -> dict
     jobs_all = sv.poisson_jobs(njobs, rate, steps=args.job_steps)
     mine = [j for k, j in enumerate(jobs_all) if k % grp.world == grp.rank]
     # each rank replays its share of the stream: arrivals keep their absolute times
-    edges = {g: args.slots_per_edge for g in ts.ensemble_grid_edges()}
+    spe = args.slots_per_edge if slots_per_edge is None else slots_per_edge
+    edges = {g: spe for g in ts.ensemble_grid_edges()}
     with sv.Server(edges, device=grp.local, hbm_budget=args.hbm_budget, epoch=args.epoch, tune=not args.no_tune,
-                   grow=not args.no_grow, group_slots=args.group_slots) as srv:
+                   grow=not args.no_grow, group_slots=args.group_slots,
+                   grow_policy=getattr(args, "grow_policy", "demand")) as srv:
         pool0, nslots, schedule = srv.pool_bytes, srv.nslots, srv.schedule
         grp.barrier()
         res = srv.run(mine, clock="wall")
@@ -210,7 +213,7 @@ def serving_leg(grp, args, rate: float, njobs: int, serial: bool = True) -> dict
     out = {"metric": "particle-steps/s (aggregate, served jobs); p50/p99 job latency",
            "value": summ["aggregate_particle_steps_per_s"], "unit": "particle-steps/s",
            "config": {"workload": f"serving_poisson{rate:g}_{njobs}jobs_{args.job_steps}steps",
-                      "initial_slots": nslots * grp.world, "slots_per_edge": args.slots_per_edge,
+                      "initial_slots": nslots * grp.world, "slots_per_edge": spe,
                       "grown_pools_rank0": grown, "group_slots": args.group_slots, "epoch_steps": args.epoch,
                       "hbm_budget_gb": args.hbm_budget / 1e9, "initial_pool_gb_per_gpu": pool0 / 1e9,
                       "peak_pool_gb_rank0": peak_bytes / 1e9, "schedule": schedule,
@@ -462,8 +465,12 @@ def run_ours(args):
     ctx.close()
     if args.workload == "blend" and not args.no_extras:
         out["ensemble"] = ensemble_leg(grp, args)
+        # each stream with the pool policy that suits its load: an overloaded stream keeps one
+        # large batched pool busy (plus growth), a stream below capacity is served fastest by
+        # pools grown per queued job
         out["serving"] = [serving_leg(grp, args, 50.0, args.jobs),
-                          serving_leg(grp, args, args.subsat_rate, args.subsat_jobs, serial=False)]
+                          serving_leg(grp, args, args.subsat_rate, args.subsat_jobs, serial=False,
+                                      slots_per_edge=args.subsat_slots_per_edge)]
         if rank == 0 and "serial" in out["serving"][0]:
             out["serving"][1]["served_over_serial"] = out["serving"][1]["value"] / out["serving"][0]["serial"]["value"]
     grp.close()
@@ -558,11 +565,15 @@ def main():
     ap.add_argument("--jobs", type=int, default=300, help="serving: number of jobs in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: mean arrivals per second")
     ap.add_argument("--job-steps", type=int, default=5000)
-    ap.add_argument("--slots-per-edge", type=int, default=0,
+    ap.add_argument("--slots-per-edge", type=int, default=12,
                     help="serving: initial slots per grid edge (0: every slot grown on demand)")
+    ap.add_argument("--subsat-slots-per-edge", type=int, default=0,
+                    help="serving: initial slots per grid edge of the below-capacity stream")
     ap.add_argument("--group-slots", type=int, default=8,
                     help="serving: largest pool grown on demand (one slot per queued job of the shape)")
     ap.add_argument("--no-grow", action="store_true", help="serving: fixed slots only")
+    ap.add_argument("--grow-policy", default="demand", choices=["demand", "load", "double"],
+                    help="serving: slots of a grown pool (see tild_serve.Server)")
     ap.add_argument("--subsat-rate", type=float, default=4.0, help="serving: the below-capacity arrival rate")
     ap.add_argument("--subsat-jobs", type=int, default=40)
     ap.add_argument("--no-extras", action="store_true", help="blend line only (no ensemble and serving legs)")

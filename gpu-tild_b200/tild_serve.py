@@ -135,6 +135,7 @@ class Server:
       job of that shape waits and the budget allows; release grown pools idle for `idle_epochs`.
       With grow, slots_per_edge may be empty: every slot is then grown on demand.
     workers: threads that step the pools of one epoch concurrently.
+    grow_policy: how many slots a grown pool gets ("demand", "load", "double"; see _pool_size).
     Slots are named by integers that stay unique for the server's lifetime.
     """
 
@@ -142,7 +143,7 @@ class Server:
                  template_of: Callable[[int], tild.System] = ts.ensemble_slot_template, device: int = 0,
                  hbm_budget: float = 80e9, epoch: int = 128, keep_positions: bool = False,
                  measure_memory: bool = True, tune: bool = False, grow: bool = False, group_slots: int = 4,
-                 idle_epochs: int = 2, workers: int = 16):
+                 idle_epochs: int = 2, workers: int = 16, grow_policy: str = "demand"):
         self.device = device
         self.epoch = int(epoch)
         self.keep_positions = keep_positions
@@ -153,6 +154,9 @@ class Server:
         self.grow = grow
         self.group_slots = int(group_slots)
         self.idle_epochs = int(idle_epochs)
+        if grow_policy not in ("demand", "load", "double"):
+            raise ValueError(f"unknown grow_policy {grow_policy}")
+        self.grow_policy = grow_policy
         self.pools: Dict[int, _Pool] = {}
         self.slot_at: Dict[int, tuple] = {}          # slot -> (pool id, index in the pool)
         self.free: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
@@ -228,11 +232,22 @@ class Server:
         pool.batch.close()
         self.pools_released += 1
 
-    def _try_grow(self, g: int, running: dict, demand: int = 0) -> bool:
-        """A pool of edge g with one slot per queued job of that shape (demand), at most
-        group_slots, if the budget allows (idle grown pools of other shapes are released first
-        when that makes room).  Returns whether slots were added."""
-        n = max(1, min(self.group_slots, demand or self.group_slots))
+    def _pool_size(self, demand: int, queued: int, shapes_waiting: int) -> int:
+        """Slots of a pool grown for a shape with `demand` queued jobs, while `queued` jobs of
+        `shapes_waiting` shapes wait in all.  "demand": one slot per queued job of the shape;
+        "load": the same while the queue is short, group_slots once it is longer than two jobs
+        per waiting shape (an overloaded stream keeps any slot busy); "double": twice the demand."""
+        if self.grow_policy == "double":
+            n = 2 * demand
+        elif self.grow_policy == "load" and queued > 2 * max(1, shapes_waiting):
+            n = self.group_slots
+        else:
+            n = demand
+        return max(1, min(self.group_slots, n or self.group_slots))
+
+    def _try_grow(self, g: int, running: dict, n: int) -> bool:
+        """A pool of n slots of edge g, if the budget allows (idle grown pools of other shapes
+        are released first when that makes room).  Returns whether slots were added."""
         caps = [max(self.capacity_of(g), self.template_of(g).ns)] * n
         need = sum(slot_bytes_estimate(g, c) for c in caps)
         known = [p for p in self.pools.values() if p.grown and p.edges[0] == g and len(p.edges) == n]
@@ -360,11 +375,14 @@ class Server:
             waiting = []
             blocked = set()                   # shapes the budget cannot grow this round
             demand = collections.Counter(edge_of(it) for it in queue)
+            queued, shapes_waiting = len(queue), len(demand)
             for item in queue:
                 g = edge_of(item)
-                if not self.free[g] and self.grow and g not in blocked and not self._try_grow(g, running, demand[g]):
+                if not self.free[g] and self.grow and g not in blocked and \
+                        not self._try_grow(g, running, self._pool_size(demand[g], queued, shapes_waiting)):
                     blocked.add(g)
                 demand[g] -= 1
+                queued -= 1
                 if self.free[g]:
                     slot = self.free[g].popleft()
                     job, r = self._start(slot, item, now())
