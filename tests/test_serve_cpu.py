@@ -178,3 +178,20 @@ def test_idle_grown_pools_release_their_memory():
     assert srv.pools_grown == 2 and srv.pools_released >= 1
     assert all(r.finished == 1 for r in res[:3]) and res[3].finished == 6
     assert len(srv.pools) <= 2
+
+
+def test_grow_policies_size_pools():
+    """Pool sizes: one slot per queued job of the shape ("demand"), the whole group once the queue
+    is long against the number of waiting shapes ("load"), twice the demand ("double")."""
+    mk = lambda pol: FakeServer({24: 1}, capacity_of=lambda g: 100, template_of=lambda g: tiny(g, 1), epoch=64,
+                                measure_memory=False, grow=True, group_slots=8, grow_policy=pol, hbm_budget=1e9)
+    d, l, x = mk("demand"), mk("load"), mk("double")
+    assert [d._pool_size(k, 40, 5) for k in (1, 3, 20)] == [1, 3, 8]
+    assert [l._pool_size(k, 4, 3) for k in (1, 3)] == [1, 3] and l._pool_size(1, 40, 5) == 8
+    assert [x._pool_size(k, 4, 3) for k in (1, 3, 6)] == [2, 6, 8]
+    try:
+        mk("sometimes")
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("an unknown policy must be rejected")
