@@ -15,11 +15,8 @@ namespace {
 
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
-__device__ __forceinline__ int ilog2c(int v) {
-  int s = 0;
-  while ((1 << s) < v) s++;
-  return s;
-}
+// ceil(log2(v)) for v >= 1
+__device__ __forceinline__ int ilog2c(int v) { return v <= 1 ? 0 : 32 - __clz(v - 1); }
 
 // Sort key of a slot: the system in the high bits, then the brick of its grid cell, then the cell
 // inside the brick (x fastest).  `brick` packs log2 of the brick edges (bits 0-3 x, 4-7 y, 8-11 z,
