@@ -515,6 +515,140 @@ __device__ __forceinline__ void gather4(const float4* __restrict__ F, const floa
     }
 }
 
+// Order 3 in 3D: the 64-node sum is split into 8 partial sums, one per (x column ix, row parity
+// pr), each over rows iy = pr, pr + 2 and the 4 z nodes in that order, combined by a fixed tree.
+// The quarter-warp gather below computes exactly this association with one lane per partial
+// (8 lanes per bead); every other order-3 3D path uses the same helpers, so all of them give the
+// same bits.
+__device__ __forceinline__ void p3_node(const float4& v, float w, float (&a)[3]) {
+  a[0] = __fmaf_rn(v.x, w, a[0]);
+  a[1] = __fmaf_rn(v.y, w, a[1]);
+  a[2] = __fmaf_rn(v.z, w, a[2]);
+}
+// a charge channel joins the type channel's sum as F + E q
+__device__ __forceinline__ float p3_join_charge(float f, float e, float q) { return __fmaf_rn(e, q, f); }
+
+// One thread's order-3 3D sum in that association; ld(ix, iy, iz) returns the node.
+template <class Ld>
+__device__ __forceinline__ void p3_partial(const float (&W)[3][4], Ld ld, int ix, int pr, float (&a)[3]) {
+  a[0] = a[1] = a[2] = 0.f;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const int iy = pr + 2 * k;
+    const float wxy = W[0][ix] * W[1][iy];
+#pragma unroll
+    for (int iz = 0; iz < 4; iz++) p3_node(ld(ix, iy, iz), wxy * W[2][iz], a);
+  }
+}
+// The tree over partials s_l, l = ix + 4 pr: ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)),
+// each pair added as soon as it exists (fewer live registers).
+template <class Ld>
+__device__ __forceinline__ void p3_sum_sequential(const float (&W)[3][4], Ld ld, float (&acc)[3]) {
+  float u[2][3];
+#pragma unroll
+  for (int pr = 0; pr < 2; pr++) {
+    float t[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      float a[3], b[3];
+      p3_partial(W, ld, 2 * h, pr, a);
+      p3_partial(W, ld, 2 * h + 1, pr, b);
+#pragma unroll
+      for (int d = 0; d < 3; d++) t[h][d] = __fadd_rn(a[d], b[d]);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) u[pr][d] = __fadd_rn(t[0][d], t[1][d]);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) acc[d] = __fadd_rn(u[0][d], u[1][d]);
+}
+
+// The order-3 3D stencil of a warp's 32 slots, 8 lanes per bead.  A request of 8 lanes reads one
+// bead's 4 x-neighbour nodes in two adjacent rows: 8 distinct 16-byte bank groups in the brick
+// and linear field layouts, so every stencil request costs the 4 L1 data wavefronts of its
+// quarters (with a bead per lane the quarters' beads collide in banks: 7.6 wavefronts per request
+// on the sorted blend, 10 once the sort is stale).  Each lane first stages its own bead's
+// weights and node offsets in shared memory; in round r quarter q sums bead 8q + r (lane
+// ix + 4 pr taking partial (ix, pr)), reduces over its 8 lanes with three xor-shuffles, and the
+// bead's own lane (8q + r) keeps the total.  Invalid slots stage offset -1 and are skipped by
+// their quarter.  Every lane of the warp must call it.
+template <bool CH>
+__device__ __forceinline__ void p3_quarter_stencil(bool valid, const int (&o)[3][4], const float (&W)[3][4],
+                                                   int tch, int qch, float q, const float4* __restrict__ F,
+                                                   float (&f)[3]) {
+  __shared__ float2 sX[kTile * 4];   // {Wx[ix], x offset + type channel}, bead slots paired by bit 3
+  __shared__ float4 sY[kTile * 2];   // {Wy[pr], Wy[pr + 2], y offsets of rows pr and pr + 2}
+  __shared__ float4 sWz[kTile];
+  __shared__ int4 sOz[kTile];
+  __shared__ float2 sQ[CH ? kTile : 1];  // {q, offset from the type channel to the charge channel}
+  const int tid = threadIdx.x, lane = tid & 31, wb = tid & ~31;
+  {
+    const int js = wb | ((lane ^ ((lane >> 3) & 1)) & 31);  // beads j and j + 8 of a half-warp: other banks
+#pragma unroll
+    for (int ix = 0; ix < 4; ix++)
+      sX[js * 4 + ix] = make_float2(W[0][ix], __int_as_float(valid ? o[0][ix] + tch : -1));
+#pragma unroll
+    for (int pr = 0; pr < 2; pr++)
+      sY[tid * 2 + pr] = make_float4(W[1][pr], W[1][pr + 2], __int_as_float(o[1][pr]), __int_as_float(o[1][pr + 2]));
+    sWz[tid] = make_float4(W[2][0], W[2][1], W[2][2], W[2][3]);
+    sOz[tid] = make_int4(o[2][0], o[2][1], o[2][2], o[2][3]);
+    if (CH) sQ[tid] = make_float2(valid ? q : 0.f, __int_as_float(qch - tch));
+  }
+  __syncwarp();
+  const int qt = lane >> 3, l8 = lane & 7, ix = l8 & 3, pr = l8 >> 2;
+#pragma unroll 1
+  for (int r = 0; r < 8; r++) {
+    const int jw = 8 * qt + r;  // bead of this quarter, within the warp
+    const int j = wb | jw;
+    const float2 xv = sX[(wb | (jw ^ ((jw >> 3) & 1))) * 4 + ix];
+    const int ox = __float_as_int(xv.y);
+    float a[3] = {0.f, 0.f, 0.f}, e[3] = {0.f, 0.f, 0.f};
+    float qj = 0.f;
+    if (ox >= 0) {  // the same for the quarter's 8 lanes
+      const float4 yv = sY[j * 2 + pr];
+      const float4 wz = sWz[j];
+      const int4 oz = sOz[j];
+      const float wy[2] = {yv.x, yv.y};
+      const int oy[2] = {__float_as_int(yv.z), __float_as_int(yv.w)};
+      const float wzv[4] = {wz.x, wz.y, wz.z, wz.w};
+      const int ozv[4] = {oz.x, oz.y, oz.z, oz.w};
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const float wxy = xv.x * wy[k];
+        const float4* row = F + (ox + oy[k]);
+#pragma unroll
+        for (int iz = 0; iz < 4; iz++) p3_node(__ldg(row + ozv[iz]), wxy * wzv[iz], a);
+      }
+      if (CH) {
+        const float2 qv = sQ[j];
+        qj = qv.x;
+        if (qj != 0.f) {
+          const int dq = __float_as_int(qv.y);
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const float wxy = xv.x * wy[k];
+            const float4* row = F + (ox + dq + oy[k]);
+#pragma unroll
+            for (int iz = 0; iz < 4; iz++) p3_node(__ldg(row + ozv[iz]), wxy * wzv[iz], e);
+          }
+        }
+      }
+    }
+    // s_l + s_(l^1), then pairs, then quads: p3_sum_sequential's tree, on every lane of the quarter
+#pragma unroll
+    for (int m = 1; m <= 4; m <<= 1)
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        a[d] = __fadd_rn(a[d], __shfl_xor_sync(0xffffffffu, a[d], m));
+        if (CH) e[d] = __fadd_rn(e[d], __shfl_xor_sync(0xffffffffu, e[d], m));
+      }
+    if (l8 == r) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) f[d] = CH && qj != 0.f ? p3_join_charge(a[d], e[d], qj) : a[d];
+    }
+  }
+}
+
 // stencil node indices -> offsets in one channel of the force field
 template <int D, int P>
 __device__ __forceinline__ void field_offsets(const int (&idx)[3][P + 1], int layout, const Geom& g,
@@ -646,6 +780,44 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : (P >= 3 ? 4 : (P >= 2 ? 3 :
     if (SPR == 0) return;
     sp = t != kPadType && finite;  // held positions are spread too
     if (t != kPadType && !finite) atomicOr(status, ST_NONFINITE_POS);
+  } else if constexpr (D == 3 && P == 3) {
+    // the quarter-warp stencil needs every lane of the warp, valid slot or not
+    const bool valid = t != kPadType && finite;
+    if (t != kPadType && !finite) atomicOr(status, ST_NONFINITE_POS);
+    const Geom& g = sd.g;
+    float W[3][4] = {};
+    int o[3][4] = {};
+    if (valid) {
+      int idx[3][4];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int b = axis_base<3>(x[d], g.dx[d], W[d]);
+#pragma unroll
+        for (int a = 0; a <= 3; a++) idx[d][a] = wrap_idx(b + a, g.nx[d], status);
+      }
+      field_offsets<3, 3>(idx, layout, g, o);
+    }
+    const long long Mb = sd.Mb;
+    float f[3] = {0.f, 0.f, 0.f};
+    p3_quarter_stencil<CH>(valid, o, W, valid ? (int)(t * Mb) : 0, (int)(sd.T * Mb), q, g4_all + sd.g4_0, f);
+    if (!valid) {
+      if (SPR == 0) return;
+    } else {
+      const int info = bond_info[i];
+      const int nb = info & 3;
+      float4 pj[3];
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++)
+        if (bb < nb) pj[bb] = pos_in[bond_nbr[3 * i + bb]];
+      const int bid = bead_id[i];
+      float4 po = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (INTEG) po = pos_io[i];
+      bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
+      if (SPR != 0) {
+        sp = isfinite(x[0]) && isfinite(x[1]) && isfinite(x[2]);
+        if (!sp) atomicOr(status, ST_NONFINITE_POS);
+      }
+    }
   } else if (t != kPadType && !finite) {
     atomicOr(status, ST_NONFINITE_POS);
     if (SPR == 0) return;  // left in place; the host reports TILD_ERR_NAN
@@ -828,13 +1000,26 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
       int lb[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < D; d++) lb[d] = rel[d] - mn[d];
-      if (CH && C && q != 0.f) {
-        float e[3] = {0.f, 0.f, 0.f};
-        box_gather4<D, P>(sbox + (long long)T * vol, W, lb, ex, ex * ey, e);
+      if constexpr (D == 3 && P == 3) {  // the association of the quarter-warp gather
+        const int exy = ex * ey;
+        const float4* bt = sbox + (long long)t * vol;
+        p3_sum_sequential(W, [&](int ix, int iy, int iz) { return bt[(lb[2] + iz) * exy + (lb[1] + iy) * ex + lb[0] + ix]; }, f);
+        if (CH && C && q != 0.f) {
+          const float4* bq = sbox + (long long)T * vol;
+          float e[3];
+          p3_sum_sequential(W, [&](int ix, int iy, int iz) { return bq[(lb[2] + iz) * exy + (lb[1] + iy) * ex + lb[0] + ix]; }, e);
 #pragma unroll
-        for (int d = 0; d < D; d++) f[d] += e[d] * q;
+          for (int d = 0; d < 3; d++) f[d] = p3_join_charge(f[d], e[d], q);
+        }
+      } else {
+        if (CH && C && q != 0.f) {
+          float e[3] = {0.f, 0.f, 0.f};
+          box_gather4<D, P>(sbox + (long long)T * vol, W, lb, ex, ex * ey, e);
+#pragma unroll
+          for (int d = 0; d < D; d++) f[d] += e[d] * q;
+        }
+        box_gather4<D, P>(sbox + (long long)t * vol, W, lb, ex, ex * ey, f);
       }
-      box_gather4<D, P>(sbox + (long long)t * vol, W, lb, ex, ex * ey, f);
     }
   } else if (ok) {
     int idx[3][P + 1];
@@ -844,13 +1029,25 @@ __global__ void __launch_bounds__(256, (P >= 4 ? 2 : 3)) k_gather_box(
       for (int a = 0; a <= P; a++) idx[d][a] = pmod(base[d] + a, g.nx[d]);
     int o[3][P + 1];
     field_offsets<D, P>(idx, TILD_FIELD_LINEAR, g, o);
-    if (CH && C && q != 0.f) {
-      float e[3] = {0.f, 0.f, 0.f};
-      gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
+    if constexpr (D == 3 && P == 3) {
+      const float4* ft = g4 + (long long)t * Mb;
+      p3_sum_sequential(W, [&](int ix, int iy, int iz) { return __ldg(ft + o[0][ix] + o[1][iy] + o[2][iz]); }, f);
+      if (CH && C && q != 0.f) {
+        const float4* fq = g4 + (long long)T * Mb;
+        float e[3];
+        p3_sum_sequential(W, [&](int ix, int iy, int iz) { return __ldg(fq + o[0][ix] + o[1][iy] + o[2][iz]); }, e);
 #pragma unroll
-      for (int d = 0; d < D; d++) f[d] += e[d] * q;
+        for (int d = 0; d < 3; d++) f[d] = p3_join_charge(f[d], e[d], q);
+      }
+    } else {
+      if (CH && C && q != 0.f) {
+        float e[3] = {0.f, 0.f, 0.f};
+        gather4<D, P>(g4 + (long long)T * Mb, W, o, e);
+#pragma unroll
+        for (int d = 0; d < D; d++) f[d] += e[d] * q;
+      }
+      gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
     }
-    gather4<D, P>(g4 + (long long)t * Mb, W, o, f);
   }
   if (!ok) return;
   bead_epilogue<D, INTEG, XW>(i, p, t, x, f, sd, g, info, nb, pj, bid, po, noise, pos_io, f_out, f_sys, s, xw);
