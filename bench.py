@@ -312,11 +312,11 @@ def step_bytes(s) -> int:
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch of the stage's kernel on this
 # workload: one ncu capture of k_gather<3,3,GJF> and k_spread_tiled<3,3> on the half-size blend
-# (--workload blend_half, one launch each inside the timed region, counters dram__bytes_read.sum
-# and dram__bytes_write.sum), doubled: the full blend has twice the beads and twice the grid
+# (--workload blend_half with the blend's tuned schedule given by --schedule, one launch each
+# inside the timed region), doubled: the full blend has twice the beads and twice the grid
 # points, and both kernels' traffic grows in proportion.
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 2 * (125391872 + 17887232), "spread": 2 * 37661440},
+    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 2 * (119605504 + 16393216), "spread": 2 * (37655296 + 768)},
 }
 
 
@@ -384,7 +384,16 @@ def run_ours(args):
     rank, local, ws = grp.rank, grp.local, grp.world
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
-    schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
+    if args.schedule:  # a fixed schedule (profiling runs): no autotuner trials before the timed region
+        t = ctx.get_tune()
+        for k, v in json.loads(args.schedule).items():
+            if k not in dict(tild.Tune._fields_):
+                raise SystemExit(f"--schedule: unknown field {k}")
+            setattr(t, k, v)
+        ctx.set_tune(t)
+        schedule = ctx.get_tune().as_dict()
+    else:
+        schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
     period = graph_period(ctx.get_tune())
     warm_and_prime(ctx, args.warmup, args.steps, period)
     grp.barrier()
@@ -581,6 +590,9 @@ def main():
     ap.add_argument("--hbm-budget", type=float, default=80e9)
     ap.add_argument("--serial-sample", type=int, default=6)
     ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner")
+    ap.add_argument("--schedule", default="",
+                    help='fixed schedule instead of the autotuner, as JSON of tild.Tune fields '
+                         '(e.g. \'{"field_layout": 1, "spread_cap": 6144}\')')
     ap.add_argument("--no-serial", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
