@@ -111,7 +111,7 @@ void free_all(tild_ctx* c) {
   for (Bucket& b : c->buckets)
     if (b.planned) {
       cufftDestroy(b.r2c);
-      cufftDestroy(b.c2r);
+      cufftDestroy(b.packed ? b.c2c : b.c2r);
     }
   for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
   c->graphs.clear();
@@ -229,7 +229,8 @@ int tild_assign_lanes(tild_ctx* c, int lanes) {
     }
     if (!b.planned) continue;
     cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
-    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") || tild_check_fft(c, cufftSetStream(b.c2r, bs), "plan stream"))
+    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") ||
+        tild_check_fft(c, cufftSetStream(b.packed ? b.c2c : b.c2r, bs), "plan stream"))
       return 1;
   }
   c->lanes = lanes;
@@ -436,6 +437,22 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
       spec += (long long)(h.T + h.C) * h.g.Mh;
       b.channels += h.T + h.C;
     }
+    // the inverse transforms pair channels when every system has an even number of them and none
+    // has a fieldphase style (those add to the planar fields between transform and interleave);
+    // each system's pair spectra follow one another, transformed in place
+    b.packed = true;
+    for (int s : b.systems) {
+      const SysHost& h = c->sys[s];
+      if ((h.T + h.C) % 2) b.packed = false;
+      for (const FieldK& f : c->fields) b.packed = b.packed && f.sys != s;
+    }
+    long long pairs = 0;
+    for (int s : b.systems) {
+      const SysHost& h = c->sys[s];
+      c->h_sys[s].inv_packed = b.packed ? 1 : 0;
+      c->h_sys[s].gkp0 = b.packed ? b.spec0 * c->D + pairs * c->D * h.g.M : 0;
+      pairs += (h.T + h.C) / 2;
+    }
   }
   c->grid_total = grid;
   c->spec_total = spec;
@@ -482,7 +499,9 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
   rc = rc ? rc : dalloc(c, &c->rho_fx, (size_t)grid, "density accumulator");
   rc = rc ? rc : dalloc(c, &c->rhok, (size_t)spec, "density spectra");
   rc = rc ? rc : dalloc(c, &c->gk, (size_t)spec * c->D, "force spectra");
-  rc = rc ? rc : dalloc(c, &c->gfield, (size_t)grid * c->D, "force fields");
+  bool any_c2r = false;  // planar force fields are only needed by buckets whose inverse is C2R
+  for (const Bucket& b : c->buckets) any_c2r = any_c2r || !b.packed;
+  rc = rc ? rc : dalloc(c, &c->gfield, any_c2r ? (size_t)grid * c->D : 1, "force fields");
   rc = rc ? rc : dalloc(c, &c->g4, (size_t)c->g4_total, "interleaved force fields");
   rc = rc ? rc : dalloc(c, &c->utab, (size_t)utab, "multiplier tables");
   rc = rc ? rc : dalloc(c, &c->virk, (size_t)virk, "virial tables");
@@ -531,7 +550,10 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
     else { n[0] = b.nx[1]; n[1] = b.nx[0]; }
     if (tild_check_fft(c, cufftPlanMany(&b.r2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, b.channels), "plan R2C"))
       return TILD_ERR_CUDA;
-    if (tild_check_fft(c, cufftPlanMany(&b.c2r, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, b.channels * c->D), "plan C2R")) {
+    const cufftResult pi = b.packed
+        ? cufftPlanMany(&b.c2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, b.channels / 2 * c->D)
+        : cufftPlanMany(&b.c2r, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, b.channels * c->D);
+    if (tild_check_fft(c, pi, b.packed ? "plan C2C" : "plan C2R")) {
       cufftDestroy(b.r2c);
       return TILD_ERR_CUDA;
     }

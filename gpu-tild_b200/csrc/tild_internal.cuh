@@ -61,6 +61,8 @@ struct SysDev {
   int active;                      // 0: skipped by the particle kernels
   long long grid0;                 // channel 0 of this system in rho / rho_fx / g4 (grid points)
   long long spec0;                 // channel 0 in rhok (half-spectrum points)
+  int inv_packed;                  // 1: inverse transforms pair channels (2c, 2c+1) into one complex C2C
+  long long gkp0;                  // with inv_packed: this system's first pair spectrum in gk (complex elements)
   long long g4_0, Mb;              // channel 0 in g4 and the per-channel stride there (>= M)
   long long utab0, ctab0, kd0;     // offsets in utab, ctab, kd
   long long step;                  // completed steps (advanced on the device)
@@ -103,12 +105,15 @@ struct SysHost {
   int sk_calls[TILD_MAX_COMPUTES] = {0};
 };
 
-struct Bucket {     // systems sharing one grid shape: one batched R2C and C2R plan
+struct Bucket {     // systems sharing one grid shape: one batched R2C plan and one batched inverse
   int nx[3];
   std::vector<int> systems;
   long long grid0 = 0, spec0 = 0;        // first channel of the bucket
   int channels = 0;
-  cufftHandle r2c = 0, c2r = 0;
+  // inverse: C2R per channel and direction, or (packed) one complex C2C per channel pair and
+  // direction whose real and imaginary parts are the pair's two real force fields
+  bool packed = false;
+  cufftHandle r2c = 0, c2r = 0, c2c = 0;
   bool planned = false;
   int cta_spec0 = 0, n_cta_spec = 0;     // the shape's range of spectrum blocks (k-space multiply)
   int cta_grid0 = 0, n_cta_grid = 0;     // and of grid blocks (interleave)

@@ -384,11 +384,40 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   kv[0] = kd[ix];
   kv[1] = kd[g.nx[0] + iy];
   kv[2] = (D == 3) ? kd[g.nx[0] + g.nx[1] + iz] : 0.f;
-  // output: -i k_d P for each channel's potential P, planar per direction (batched C2R input)
-  float2* gk = gk_all + sd.spec0 * D;
+  // output: -i k_d P for each channel's potential P, planar per direction (batched C2R input); or,
+  // with inv_packed, W = G_a + i G_b for each channel pair (a, b) = (2p, 2p + 1) over the full
+  // spectrum (batched C2C input): W(k) here, and W(-k) = conj(G_a) + i conj(G_b) when -k lies
+  // outside the half spectrum (0 < ix < nx/2), so the complex inverse returns g_a + i g_b
+  const bool packed = sd.inv_packed;
+  float2* gk = packed ? gk_all + sd.gkp0 : gk_all + sd.spec0 * D;
+  long long fk = 0, fmk = 0;
+  bool mirror = false;
+  if (packed) {
+    const int nx = g.nx[0], ny = g.nx[1], nz = D == 3 ? g.nx[2] : 1;
+    fk = ((long long)iz * ny + iy) * nx + ix;
+    fmk = ((long long)(iz ? nz - iz : 0) * ny + (iy ? ny - iy : 0)) * nx + (ix ? nx - ix : 0);
+    mirror = ix > 0 && 2 * ix != nx;
+  }
+  const long long M = g.M;
+  float2 held = make_float2(0.f, 0.f);
   auto store = [&](int ch, float2 P) {
+    if (!packed) {
 #pragma unroll
-    for (int d = 0; d < D; d++) gk[((long long)ch * D + d) * Mh + h] = make_float2(kv[d] * P.y, -kv[d] * P.x);
+      for (int d = 0; d < D; d++) gk[((long long)ch * D + d) * Mh + h] = make_float2(kv[d] * P.y, -kv[d] * P.x);
+      return;
+    }
+    if (!(ch & 1)) {  // channels come in order; the pair is written with its odd channel
+      held = P;
+      return;
+    }
+    float2* W = gk + (long long)(ch >> 1) * D * M;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const float2 ga = make_float2(kv[d] * held.y, -kv[d] * held.x);
+      const float2 gb = make_float2(kv[d] * P.y, -kv[d] * P.x);
+      W[d * M + fk] = make_float2(ga.x - gb.y, ga.y + gb.x);
+      if (mirror) W[d * M + fmk] = make_float2(ga.x + gb.y, gb.x - ga.y);
+    }
   };
   if (NT > 0) {
     constexpr int NA = NT > 0 ? NT : 1;
@@ -457,8 +486,8 @@ __global__ void k_fieldphase_apply(float* __restrict__ gfield, const float* __re
 // (Writing the float4 field from strided inverse transforms instead was measured slower at 128^3
 // and no faster on small grids.)
 template <int D>
-__global__ void k_interleave(const float* __restrict__ planar_all, float4* __restrict__ g4_all,
-                             const int* __restrict__ cta_sys, const int* __restrict__ blk0,
+__global__ void k_interleave(const float* __restrict__ planar_all, const float2* __restrict__ pairs_all,
+                             float4* __restrict__ g4_all, const int* __restrict__ cta_sys, const int* __restrict__ blk0,
                              const SysDev* __restrict__ sysd, int layout, int blk_off) {
   const int blk = blockIdx.x + blk_off;
   const int s = cta_sys[blk];
@@ -478,6 +507,16 @@ __global__ void k_interleave(const float* __restrict__ planar_all, float4* __res
   const float* planar = planar_all + sd.grid0 * D;
   float4* g4 = g4_all + sd.g4_0;
   const int nch = sd.T + sd.C;
+  if (sd.inv_packed) {  // pair p's direction d is one complex field: real part channel 2p, imaginary 2p + 1
+    const float2* z = pairs_all + sd.gkp0;
+    for (int p = 0; p < nch / 2; p++) {
+      const float2* src = z + (long long)p * D * M + m;
+      const float2 vx = src[0], vy = src[M], vz = D == 3 ? src[2 * M] : make_float2(0.f, 0.f);
+      g4[(long long)(2 * p) * sd.Mb + dst] = make_float4(vx.x, vy.x, vz.x, 0.f);
+      g4[(long long)(2 * p + 1) * sd.Mb + dst] = make_float4(vx.y, vy.y, vz.y, 0.f);
+    }
+    return;
+  }
   for (int ch = 0; ch < nch; ch++) {
     const float* src = planar + (long long)ch * D * M + m;
     g4[(long long)ch * sd.Mb + dst] = make_float4(src[0], src[M], D == 3 ? src[2 * M] : 0.f, 0.f);
@@ -1189,9 +1228,11 @@ void launch_interleave(tild_ctx* c, cudaStream_t st, int off, int n) {
   if (n == 0) return;
   int* blk0 = c->cta_grid + c->n_cta_grid;
   if (c->D == 3)
-    k_interleave<3><<<n, 256, 0, st>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout, off);
+    k_interleave<3><<<n, 256, 0, st>>>(c->gfield, reinterpret_cast<const float2*>(c->gk), c->g4, c->cta_grid, blk0,
+                                       c->d_sys, c->field_layout, off);
   else
-    k_interleave<2><<<n, 256, 0, st>>>(c->gfield, c->g4, c->cta_grid, blk0, c->d_sys, c->field_layout, off);
+    k_interleave<2><<<n, 256, 0, st>>>(c->gfield, reinterpret_cast<const float2*>(c->gk), c->g4, c->cta_grid, blk0,
+                                       c->d_sys, c->field_layout, off);
 }
 
 // k-space multiply over spectrum blocks [off, off + n) (all of them by default) on stream st
@@ -1219,6 +1260,14 @@ int fork(tild_ctx* c) {
   for (int k = 0; k < c->lanes; k++)
     if (tild_check(c, cudaStreamWaitEvent(c->aux[k], c->ev_fork, 0), "fork wait")) return 1;
   return 0;
+}
+
+// the bucket's batched inverse transform: C2R per channel and direction, or C2C per channel pair
+int exec_inverse(tild_ctx* c, const Bucket& b) {
+  if (b.packed)
+    return tild_check_fft(c, cufftExecC2C(b.c2c, c->gk + b.spec0 * c->D, c->gk + b.spec0 * c->D, CUFFT_INVERSE),
+                          "C2C");  // in place: the interleave reads the pair fields from gk
+  return tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R");
 }
 
 int join(tild_ctx* c) {
@@ -1261,7 +1310,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
         if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
         if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
         else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
-        if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+        if (exec_inverse(c, b))
           return TILD_ERR_CUDA;
         launch_interleave(c, bs, b.cta_grid0, b.n_cta_grid);
         c->launches += 2;
@@ -1298,7 +1347,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
       if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
       else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
       c->launches++;
-      if (tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+      if (exec_inverse(c, b))
         return TILD_ERR_CUDA;
       if (c->fields.empty()) {  // fieldphase edits the planar fields first when present
         launch_interleave(c, bs, b.cta_grid0, b.n_cta_grid);
@@ -1330,7 +1379,7 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
   if (fork(c)) return TILD_ERR_CUDA;
   for (size_t bi = 0; bi < c->buckets.size(); bi++) {
     const Bucket& b = c->buckets[bi];
-    if (on[bi] && tild_check_fft(c, cufftExecC2R(b.c2r, c->gk + b.spec0 * c->D, c->gfield + b.grid0 * c->D), "C2R"))
+    if (on[bi] && exec_inverse(c, b))
       return TILD_ERR_CUDA;
   }
   if (join(c)) return TILD_ERR_CUDA;

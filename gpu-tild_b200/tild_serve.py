@@ -103,11 +103,12 @@ def device_free_bytes(device: int) -> int:
 def slot_bytes_estimate(g: int, capacity: int) -> int:
     """Device bytes of one slot of grid edge g (diblock: two density channels, three gaussian
     styles) from the engine's layout: per grid point and channel 8 (fixed-point) + 4 (density) +
-    12 (planar field) + 16 (float4 field) bytes and 32 bytes of half spectra, the multiplier and
-    virial tables, and about 100 bytes per bead of capacity.  Used when the footprint is not
-    measured on the device."""
+    16 (float4 field) bytes and 16 bytes of half spectra (the two channels' inverse transforms run
+    as one complex transform in the force spectra, so no planar fields), the multiplier and virial
+    tables, and about 100 bytes per bead of capacity.  Used when the footprint is not measured on
+    the device."""
     M = g ** 3
-    return int(2 * 40 * M + 2 * 16 * M + 3 * 2 * M + 3 * 6 * 4 * M + 100 * capacity)
+    return int(2 * 28 * M + 2 * 16 * M + 3 * 2 * M + 3 * 6 * 4 * M + 100 * capacity)
 
 
 class _Pool:
