@@ -422,15 +422,17 @@ def run_ours(args):
     x_out = tild.HostArray((s.ns, s.dim))
     def e2e_run():
         ctx.set_state(x_in.array)
-        done, reads = 0, 0
+        done, reads, ticket = 0, 0, None
         while done < e2e_steps:
             n = min(log_freq, e2e_steps - done)
             ctx.step(n)
             done += n
+            if done == e2e_steps:   # final positions to the host, copied while the last record is computed
+                ticket = ctx.snapshot_async(x_out.array, None)
             if done % log_freq == 0 or done == e2e_steps:   # a record every 128 steps and at the end
                 ctx.observables()
                 reads += 1
-        ctx.snapshot_wait(ctx.snapshot_async(x_out.array, None))   # final positions to the host
+        ctx.snapshot_wait(ticket)
         return reads
 
     # one untimed rehearsal: the first observables call allocates the reduction scratch, the first
