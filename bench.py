@@ -88,6 +88,17 @@ def ensemble(n: int = 256):
     return [ts.ensemble_member(i) for i in range(n)]
 
 
+def apply_schedule(engine, spec: str) -> dict:
+    """Sets the tild.Tune fields given as JSON on a context or batch (instead of the autotuner)."""
+    t = engine.get_tune()
+    for k, v in json.loads(spec).items():
+        if k not in dict(tild.Tune._fields_):
+            raise SystemExit(f"--schedule: unknown field {k}")
+        setattr(t, k, v)
+    engine.set_tune(t)
+    return engine.get_tune().as_dict()
+
+
 def ensemble_leg(grp, args) -> dict:
     """Batched ensemble: 256 independent diblock systems (box L ~ U(12, 24) snapped to dx = 0.5,
     grids 24^3..48^3, N ~ U{10..40}, f_A ~ U(0.3, 0.7), chi N ~ U(10, 30), rho0 = 5) advanced
@@ -97,7 +108,7 @@ def ensemble_leg(grp, args) -> dict:
     mine = tild_dist.shard([s.ns for s in systems], grp.rank, grp.world)
     local = [systems[i] for i in mine]
     B = tild.Batch(local, device=grp.local)
-    schedule = None if args.no_tune else B.autotune(trial_steps=64)
+    schedule = apply_schedule(B, args.schedule) if args.schedule else (None if args.no_tune else B.autotune(trial_steps=64))
     steps = args.steps
     warm_and_prime(B, args.warmup, steps, graph_period(B.get_tune()))
     grp.barrier()
@@ -385,13 +396,7 @@ def run_ours(args):
     s, wname = make_system(args.workload)
     ctx = tild.Context(s, device=local)
     if args.schedule:  # a fixed schedule (profiling runs): no autotuner trials before the timed region
-        t = ctx.get_tune()
-        for k, v in json.loads(args.schedule).items():
-            if k not in dict(tild.Tune._fields_):
-                raise SystemExit(f"--schedule: unknown field {k}")
-            setattr(t, k, v)
-        ctx.set_tune(t)
-        schedule = ctx.get_tune().as_dict()
+        schedule = apply_schedule(ctx, args.schedule)
     else:
         schedule = None if args.no_tune else ctx.autotune(trial_steps=64)
     period = graph_period(ctx.get_tune())
