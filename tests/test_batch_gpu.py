@@ -37,6 +37,29 @@ def test_batch_forces_match_single_and_oracle():
         assert rel_l2(fb[i], fo) < FORCE_RTOL, i
 
 
+def test_batch_mixes_paired_and_per_channel_inverses():
+    """A grid shape whose systems all have an even channel count and no fieldphase takes the paired
+    complex inverse; a fieldphase system turns its whole shape to per-channel C2R.  Here the 16^3
+    shape holds a plain diblock (paired when alone) and a fieldphase system, the other shapes stay
+    paired: every system must still match its single-system run and the oracle."""
+    a = small_diblock(3, 1, nx=(16, 16, 16), box=(8.0, 8.0, 8.0), seed=1)
+    f = small_diblock(3, 1, nx=(16, 16, 16), box=(8.5, 8.5, 8.5), n_chains=90, seed=4)
+    f.styles = f.styles + [tild.Style(tild.STYLE_FIELDPHASE, 0, 1, 0.7, phase=0, dir=1, n_periods=2)]
+    b = small_diblock(3, 1, nx=(12, 14, 16), box=(6.0, 7.0, 8.0), n_chains=70, seed=2)
+    d = charged_system()
+    systems = [a, f, b, d]
+    with tild.Batch(systems) as B:
+        fb = [B.forces(i) for i in range(len(systems))]
+        rb = [B.density(i) for i in range(len(systems))]
+    for i, s in enumerate(systems):
+        with tild.Context(s) as c:
+            fs = c.forces()
+            rs = c.density()
+        assert np.array_equal(rb[i], rs), f"system {i}: densities differ"
+        assert rel_l2(fb[i], fs) < 1e-6, i
+        assert rel_l2(fb[i], oracle.Oracle(s).forces(s.x, 0)) < FORCE_RTOL, i
+
+
 def test_batch_steps_match_single_runs():
     systems = mixed_systems()
     with tild.Batch(systems) as B:
