@@ -110,7 +110,7 @@ void free_all(tild_ctx* c) {
   if (c->snap_stream) cudaStreamDestroy(c->snap_stream);
   for (Bucket& b : c->buckets)
     if (b.planned) {
-      cufftDestroy(b.r2c);
+      cufftDestroy(b.fwd_packed ? b.c2c_fwd : b.r2c);
       cufftDestroy(b.packed ? b.c2c : b.c2r);
     }
   for (auto& ge : c->graphs) cudaGraphExecDestroy(ge.exec);
@@ -229,7 +229,7 @@ int tild_assign_lanes(tild_ctx* c, int lanes) {
     }
     if (!b.planned) continue;
     cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
-    if (tild_check_fft(c, cufftSetStream(b.r2c, bs), "plan stream") ||
+    if (tild_check_fft(c, cufftSetStream(b.fwd_packed ? b.c2c_fwd : b.r2c, bs), "plan stream") ||
         tild_check_fft(c, cufftSetStream(b.packed ? b.c2c : b.c2r, bs), "plan stream"))
       return 1;
   }
@@ -446,11 +446,16 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
       if ((h.T + h.C) % 2) b.packed = false;
       for (const FieldK& f : c->fields) b.packed = b.packed && f.sys != s;
     }
+    // the forward transforms pair them the same way when the bucket's densities start on a complex
+    // boundary (they are read as complex pairs); the pair spectra follow one another in rhok
+    b.fwd_packed = b.packed && b.grid0 % 2 == 0;
     long long pairs = 0;
     for (int s : b.systems) {
       const SysHost& h = c->sys[s];
       c->h_sys[s].inv_packed = b.packed ? 1 : 0;
       c->h_sys[s].gkp0 = b.packed ? b.spec0 * c->D + pairs * c->D * h.g.M : 0;
+      c->h_sys[s].fwd_packed = b.fwd_packed ? 1 : 0;
+      c->h_sys[s].rkp0 = b.fwd_packed ? b.spec0 + pairs * h.g.M : 0;
       pairs += (h.T + h.C) / 2;
     }
   }
@@ -548,13 +553,15 @@ int engine_create(const tild_config* cfgs, int nsys, int device, tild_ctx* c, co
     int n[3];
     if (c->D == 3) { n[0] = b.nx[2]; n[1] = b.nx[1]; n[2] = b.nx[0]; }
     else { n[0] = b.nx[1]; n[1] = b.nx[0]; }
-    if (tild_check_fft(c, cufftPlanMany(&b.r2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, b.channels), "plan R2C"))
-      return TILD_ERR_CUDA;
+    const cufftResult pf = b.fwd_packed
+        ? cufftPlanMany(&b.c2c_fwd, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, b.channels / 2)
+        : cufftPlanMany(&b.r2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, b.channels);
+    if (tild_check_fft(c, pf, b.fwd_packed ? "plan C2C forward" : "plan R2C")) return TILD_ERR_CUDA;
     const cufftResult pi = b.packed
         ? cufftPlanMany(&b.c2c, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, b.channels / 2 * c->D)
         : cufftPlanMany(&b.c2r, c->D, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, b.channels * c->D);
     if (tild_check_fft(c, pi, b.packed ? "plan C2C" : "plan C2R")) {
-      cufftDestroy(b.r2c);
+      cufftDestroy(b.fwd_packed ? b.c2c_fwd : b.r2c);
       return TILD_ERR_CUDA;
     }
     b.planned = true;
@@ -870,7 +877,13 @@ int sys_density(tild_ctx* c, int s, float* rho) {
   const SysHost& h = c->sys[s];
   if (!h.have_forces) return set_err(c, TILD_ERR_STATE, "no force evaluation yet");
   cudaSetDevice(c->device);
-  if (tild_check(c, cudaMemcpyAsync(rho, c->rho + h.grid0, sizeof(float) * (size_t)(h.T + h.C) * h.g.M, cudaMemcpyDeviceToHost, c->stream), "download rho") ||
+  const float* src = c->rho + h.grid0;
+  if (c->h_sys[s].fwd_packed) {  // paired layout: planar channels staged in the force-field scratch first
+    float* planar = reinterpret_cast<float*>(c->gk) + h.grid0;
+    if (tild_density_planar(c, s, planar, c->stream)) return TILD_ERR_CUDA;
+    src = planar;
+  }
+  if (tild_check(c, cudaMemcpyAsync(rho, src, sizeof(float) * (size_t)(h.T + h.C) * h.g.M, cudaMemcpyDeviceToHost, c->stream), "download rho") ||
       tild_check(c, cudaStreamSynchronize(c->stream), "sync rho"))
     return TILD_ERR_CUDA;
   return TILD_OK;
@@ -1231,9 +1244,7 @@ int sys_snapshot_async(tild_ctx* c, int s, float* x, float* rho, int64_t* ticket
                                                              h.ns_pad, h.D, sl.dx);
     c->launches++;
   }
-  if (rho && tild_check(c, cudaMemcpyAsync(sl.drho, c->rho + h.grid0, nr * sizeof(float), cudaMemcpyDeviceToDevice,
-                                           c->stream), "snapshot rho"))
-    return TILD_ERR_CUDA;
+  if (rho && tild_density_planar(c, s, sl.drho, c->stream)) return TILD_ERR_CUDA;
   if (tild_check(c, cudaEventRecord(sl.captured, c->stream), "snapshot event") ||
       tild_check(c, cudaStreamWaitEvent(c->snap_stream, sl.captured, 0), "snapshot wait"))
     return TILD_ERR_CUDA;

@@ -63,6 +63,9 @@ struct SysDev {
   long long spec0;                 // channel 0 in rhok (half-spectrum points)
   int inv_packed;                  // 1: inverse transforms pair channels (2c, 2c+1) into one complex C2C
   long long gkp0;                  // with inv_packed: this system's first pair spectrum in gk (complex elements)
+  int fwd_packed;                  // 1: densities of channels (2c, 2c+1) are stored as one complex field
+                                   //    (real, imaginary) and take one forward C2C
+  long long rkp0;                  // with fwd_packed: this system's first pair spectrum in rhok (complex elements)
   long long g4_0, Mb;              // channel 0 in g4 and the per-channel stride there (>= M)
   long long utab0, ctab0, kd0;     // offsets in utab, ctab, kd
   long long step;                  // completed steps (advanced on the device)
@@ -113,7 +116,8 @@ struct Bucket {     // systems sharing one grid shape: one batched R2C plan and 
   // inverse: C2R per channel and direction, or (packed) one complex C2C per channel pair and
   // direction whose real and imaginary parts are the pair's two real force fields
   bool packed = false;
-  cufftHandle r2c = 0, c2r = 0, c2c = 0;
+  bool fwd_packed = false;               // the forward transforms pair channels too (out of place C2C)
+  cufftHandle r2c = 0, c2r = 0, c2c = 0, c2c_fwd = 0;
   bool planned = false;
   int cta_spec0 = 0, n_cta_spec = 0;     // the shape's range of spectrum blocks (k-space multiply)
   int cta_grid0 = 0, n_cta_grid = 0;     // and of grid blocks (interleave)
@@ -305,6 +309,13 @@ __device__ __forceinline__ int tild_field_off(int layout, int d, int n, const Ge
 }
 __device__ __forceinline__ int tild_type_of(float w) { return __float_as_int(w) & 0xff; }
 
+// One channel of a paired density spectrum: Z = X_a + i X_b with X_a, X_b the spectra of two real
+// fields, z = Z(k), zm = Z(-k); X_a(k) = (z + conj zm) / 2 (second = 0), X_b(k) = (z - conj zm) / 2i.
+__device__ __forceinline__ float2 pair_unpack(float2 z, float2 zm, int second) {
+  return second ? make_float2(0.5f * (z.y + zm.y), 0.5f * (zm.x - z.x))
+                : make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+}
+
 // spline_get_weights (device_grid_utils.cu:3-49), FP32, including the order-4 quirk
 // sx3 = sx2*sx2 of line 39.
 template <int P>
@@ -421,6 +432,8 @@ __host__ __device__ inline float ramp_ratio(const SysDev& d, int k, long long st
 int tild_build_tables(tild_ctx* c, int s);            // tild_tables.cu
 int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys);   // tild_step.cu
 int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bool interleaved, bool gathered);
+int tild_density_planar(tild_ctx* c, int s, float* dst, cudaStream_t st);                 // tild_step.cu
+const float2* tild_half_spectra(tild_ctx* c, int s);                                     // tild_step.cu
 int tild_obs_compute(tild_ctx* c, int s, tild_obs* o); // tild_obs.cu
 int tild_sk_acc_run(tild_ctx* c, int s, int slot, int type);
 int tild_table_scratch(tild_ctx* c);

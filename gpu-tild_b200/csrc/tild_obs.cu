@@ -353,7 +353,7 @@ int tild_obs_compute(tild_ctx* c, int si, tild_obs* o) {
   o->step = h.forces_step;
   const int nblocks = 296;
   if (tild_ensure_red(c, 7, nblocks)) return TILD_ERR_OOM;
-  const float2* rk = reinterpret_cast<const float2*>(c->rhok) + h.spec0;
+  const float2* rk = tild_half_spectra(c, si);  // per-channel half spectra of the last force evaluation
   double upe = 0.0;
   for (size_t k = 0; k < h.fft_cfg.size(); k++) {
     const int ci = h.fft_cfg[k];
@@ -409,9 +409,9 @@ int tild_sk_acc_run(tild_ctx* c, int si, int slot, int type) {
       return TILD_ERR_CUDA;
     h.sk_calls[slot] = 0;
   }
-  k_sk_acc<<<nblk(h.g.Mh, 256), 256, 0, c->stream>>>(
-      reinterpret_cast<double2*>(h.sk[slot]),
-      reinterpret_cast<const float2*>(c->rhok) + h.spec0 + (long long)type * h.g.Mh, h.g.Mh, 1.0 / (double)h.g.M);
+  k_sk_acc<<<nblk(h.g.Mh, 256), 256, 0, c->stream>>>(reinterpret_cast<double2*>(h.sk[slot]),
+                                                      tild_half_spectra(c, si) + (long long)type * h.g.Mh, h.g.Mh,
+                                                      1.0 / (double)h.g.M);
   c->launches++;
   h.sk_calls[slot]++;
   return tild_check(c, cudaGetLastError(), "sk accumulate") ? TILD_ERR_CUDA : TILD_OK;

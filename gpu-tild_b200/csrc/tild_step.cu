@@ -341,6 +341,48 @@ __global__ void k_fix_to_float(unsigned long long* __restrict__ fx, float* __res
   fx[k] = 0ull;
 }
 
+// The same conversion for a grid shape whose channels are paired: channels 2p and 2p + 1 of node m
+// become the complex value (rho_2p, rho_2p+1) at pair p, the forward C2C's input.
+__global__ void k_fix_to_pairs(unsigned long long* __restrict__ fx, float2* __restrict__ pairs, long long npairs,
+                               long long M) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= npairs * M) return;
+  const long long p = k / M, m = k - p * M;
+  unsigned long long* a = fx + 2 * p * M + m;
+  const long long va = (long long)a[0], vb = (long long)a[M];
+  pairs[k] = make_float2((float)((double)va * kInvFix), (float)((double)vb * kInvFix));
+  a[0] = 0ull;
+  a[M] = 0ull;
+}
+
+// paired density spectra -> per-channel half spectra (the R2C layout, for the observables and S(k)):
+// one thread per half-spectrum point, every pair of the system
+__global__ void k_unpack_half(const float2* __restrict__ z, float2* __restrict__ half, int npairs, Geom g, int D) {
+  const long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (h >= g.Mh) return;
+  const unsigned hu = (unsigned)h, rr = hu / (unsigned)g.nxh;
+  const int ix = (int)(hu - rr * (unsigned)g.nxh), iy = (int)(rr % (unsigned)g.nx[1]), iz = (int)(rr / (unsigned)g.nx[1]);
+  const int nx = g.nx[0], ny = g.nx[1], nz = D == 3 ? g.nx[2] : 1;
+  const long long fk = ((long long)iz * ny + iy) * nx + ix;
+  const long long fmk = ((long long)(iz ? nz - iz : 0) * ny + (iy ? ny - iy : 0)) * nx + (ix ? nx - ix : 0);
+  for (int p = 0; p < npairs; p++) {
+    const float2 a = z[(long long)p * g.M + fk], am = z[(long long)p * g.M + fmk];
+    half[(long long)(2 * p) * g.Mh + h] = pair_unpack(a, am, 0);
+    half[(long long)(2 * p + 1) * g.Mh + h] = pair_unpack(a, am, 1);
+  }
+}
+
+// paired densities -> planar channels (density reads and snapshots): n = pairs x M
+__global__ void k_pairs_to_planar(const float2* __restrict__ pairs, float* __restrict__ planar, long long npairs,
+                                  long long M) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= npairs * M) return;
+  const long long p = k / M, m = k - p * M;
+  const float2 v = pairs[k];
+  planar[2 * p * M + m] = v.x;
+  planar[(2 * p + 1) * M + m] = v.y;
+}
+
 // ---------------------------------------------------------------------------------------------
 // k-space multiply (replaces d_prepareForceKSpace, device_array_utils.cu:298-312, for every
 // style and side, and d_prepareElectrostaticPotential / d_prepareElectricField :199-241)
@@ -388,17 +430,25 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
   // with inv_packed, W = G_a + i G_b for each channel pair (a, b) = (2p, 2p + 1) over the full
   // spectrum (batched C2C input): W(k) here, and W(-k) = conj(G_a) + i conj(G_b) when -k lies
   // outside the half spectrum (0 < ix < nx/2), so the complex inverse returns g_a + i g_b
-  const bool packed = sd.inv_packed;
+  const bool packed = sd.inv_packed, fwd = sd.fwd_packed;
   float2* gk = packed ? gk_all + sd.gkp0 : gk_all + sd.spec0 * D;
-  long long fk = 0, fmk = 0;
+  long long fk = 0, fmk = 0;  // full-spectrum indices of k and -k
   bool mirror = false;
-  if (packed) {
+  if (packed || fwd) {
     const int nx = g.nx[0], ny = g.nx[1], nz = D == 3 ? g.nx[2] : 1;
     fk = ((long long)iz * ny + iy) * nx + ix;
     fmk = ((long long)(iz ? nz - iz : 0) * ny + (iy ? ny - iy : 0)) * nx + (ix ? nx - ix : 0);
     mirror = ix > 0 && 2 * ix != nx;
   }
   const long long M = g.M;
+  // a channel's density spectrum at k: the R2C output, or, with fwd_packed, from its pair's
+  // spectrum Z = X_2p + i X_2p+1: X_2p = (Z(k) + conj Z(-k)) / 2, X_2p+1 = (Z(k) - conj Z(-k)) / 2i
+  const float2* zpairs = rhok_all + sd.rkp0;
+  auto rho_hat = [&](int ch) -> float2 {
+    if (!fwd) return rhok[(long long)ch * Mh + h];
+    const float2* zp = zpairs + (long long)(ch >> 1) * M;
+    return pair_unpack(zp[fk], zp[fmk], ch & 1);
+  };
   float2 held = make_float2(0.f, 0.f);
   auto store = [&](int ch, float2 P) {
     if (!packed) {
@@ -424,7 +474,7 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
     float2 rk[NA], phi[NA];
 #pragma unroll
     for (int t = 0; t < NA; t++) {
-      rk[t] = (t < T) ? rhok[(long long)t * Mh + h] : make_float2(0.f, 0.f);
+      rk[t] = (t < T) ? rho_hat(t) : make_float2(0.f, 0.f);
       phi[t] = make_float2(0.f, 0.f);
     }
     for (int k = 0; k < nfft; k++) {
@@ -454,14 +504,14 @@ __global__ void __launch_bounds__(256) k_kmul(const float2* __restrict__ rhok_al
     for (int k = 0; k < nfft; k++) {
       const float u = utab[(long long)k * Mh] * s_scale[k];
       const int a = s_ab[k] & 0xff, b = s_ab[k] >> 8;
-      const float2 ra = rhok[(long long)a * Mh + h], rb = rhok[(long long)b * Mh + h];
+      const float2 ra = rho_hat(a), rb = rho_hat(b);
       phi[a].x += u * rb.x; phi[a].y += u * rb.y;
       phi[b].x += u * ra.x; phi[b].y += u * ra.y;
     }
     for (int t = 0; t < T; t++) store(t, phi[t]);
   }
   if (C) {
-    const float2 rc = rhok[(long long)T * Mh + h];
+    const float2 rc = rho_hat(T);
     const float cm = ctab_all[sd.ctab0 + h];
     const float2 pc = make_float2(cm * rc.x, cm * rc.y);
     store(T, pc);
@@ -1262,6 +1312,30 @@ int fork(tild_ctx* c) {
   return 0;
 }
 
+// the bucket's fixed-point densities to FP32 (clearing the accumulator): planar channels, or
+// complex channel pairs when its forward transform is paired
+void launch_fix(tild_ctx* c, const Bucket& b, cudaStream_t st) {
+  const long long M = (long long)b.nx[0] * b.nx[1] * b.nx[2];
+  if (b.fwd_packed) {
+    const long long np = b.channels / 2;
+    k_fix_to_pairs<<<nblk(np * M, 256), 256, 0, st>>>(c->rho_fx + b.grid0, reinterpret_cast<float2*>(c->rho + b.grid0),
+                                                      np, M);
+  } else {
+    k_fix_to_float<<<nblk((long long)b.channels * M, 256), 256, 0, st>>>(c->rho_fx + b.grid0, c->rho + b.grid0,
+                                                                         (long long)b.channels * M);
+  }
+  c->launches++;
+}
+
+// the bucket's batched forward transform: R2C per channel, or C2C per channel pair (out of place,
+// the pair spectra into rhok; the paired real-space densities stay for density reads)
+int exec_forward(tild_ctx* c, const Bucket& b) {
+  if (b.fwd_packed)
+    return tild_check_fft(c, cufftExecC2C(b.c2c_fwd, reinterpret_cast<cufftComplex*>(c->rho + b.grid0),
+                                          c->rhok + b.spec0, CUFFT_FORWARD), "C2C forward");
+  return tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C");
+}
+
 // the bucket's batched inverse transform: C2R per channel and direction, or C2C per channel pair
 int exec_inverse(tild_ctx* c, const Bucket& b) {
   if (b.packed)
@@ -1303,11 +1377,9 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
         else dispatch_p_spread<2>(c, r);
         c->launches++;
       }
-      const long long n = (long long)b.channels * b.nx[0] * b.nx[1] * b.nx[2];
-      k_fix_to_float<<<nblk(n, 256), 256, 0, bs>>>(c->rho_fx + b.grid0, c->rho + b.grid0, n);
-      c->launches++;
+      launch_fix(c, b, bs);
       if (on[bi]) {
-        if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+        if (exec_forward(c, b)) return TILD_ERR_CUDA;
         if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
         else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
         if (exec_inverse(c, b))
@@ -1339,11 +1411,9 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
     for (size_t bi = 0; bi < c->buckets.size(); bi++) {
       const Bucket& b = c->buckets[bi];
       cudaStream_t bs = b.lane >= 0 ? c->aux[b.lane] : c->stream;
-      const long long n = (long long)b.channels * b.nx[0] * b.nx[1] * b.nx[2];
-      k_fix_to_float<<<nblk(n, 256), 256, 0, bs>>>(c->rho_fx + b.grid0, c->rho + b.grid0, n);
-      c->launches++;
+      launch_fix(c, b, bs);
       if (!on[bi]) continue;
-      if (tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C")) return TILD_ERR_CUDA;
+      if (exec_forward(c, b)) return TILD_ERR_CUDA;
       if (c->D == 3) launch_kmul<3>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
       else launch_kmul<2>(c, integrate, bs, b.cta_spec0, b.n_cta_spec);
       c->launches++;
@@ -1359,15 +1429,20 @@ int tild_run_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys) {
     return tild_finish_forces(c, integrate, f_bead, f_sys, c->fields.empty(), false);
   }
   tild_mark(c, STAGE_ZERO);
-  k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
-  c->launches++;
+  bool any_fwd_packed = false;
+  for (const Bucket& b : c->buckets) any_fwd_packed = any_fwd_packed || b.fwd_packed;
+  if (any_fwd_packed) {  // paired shapes convert into their own layout
+    for (const Bucket& b : c->buckets) launch_fix(c, b, c->stream);
+  } else {
+    k_fix_to_float<<<nblk(c->grid_total, 256), 256, 0, c->stream>>>(c->rho_fx, c->rho, c->grid_total);
+    c->launches++;
+  }
   if (tild_check(c, cudaGetLastError(), "spread")) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_R2C);
   if (fork(c)) return TILD_ERR_CUDA;
   for (size_t bi = 0; bi < c->buckets.size(); bi++) {
     const Bucket& b = c->buckets[bi];
-    if (on[bi] && tild_check_fft(c, cufftExecR2C(b.r2c, c->rho + b.grid0, c->rhok + b.spec0), "R2C"))
-      return TILD_ERR_CUDA;
+    if (on[bi] && exec_forward(c, b)) return TILD_ERR_CUDA;
   }
   if (join(c)) return TILD_ERR_CUDA;
   tild_mark(c, STAGE_KMUL);
@@ -1427,4 +1502,33 @@ int tild_finish_forces(tild_ctx* c, bool integrate, float* f_bead, int f_sys, bo
     h.have_forces = true;
   }
   return TILD_OK;
+}
+
+// A system's densities as planar FP32 channels [(T + C)][M] into dst (device memory) on stream st:
+// a copy, or the de-interleave of its paired layout.
+int tild_density_planar(tild_ctx* c, int s, float* dst, cudaStream_t st) {
+  const SysHost& h = c->sys[s];
+  const long long M = h.g.M;
+  if (c->h_sys[s].fwd_packed) {
+    const long long np = (h.T + h.C) / 2;
+    k_pairs_to_planar<<<nblk(np * M, 256), 256, 0, st>>>(reinterpret_cast<const float2*>(c->rho + h.grid0), dst, np, M);
+    c->launches++;
+    return tild_check(c, cudaGetLastError(), "densities to planar") ? TILD_ERR_CUDA : TILD_OK;
+  }
+  return tild_check(c, cudaMemcpyAsync(dst, c->rho + h.grid0, sizeof(float) * (size_t)(h.T + h.C) * M,
+                                       cudaMemcpyDeviceToDevice, st), "copy densities") ? TILD_ERR_CUDA : TILD_OK;
+}
+
+// A system's density half spectra in the R2C layout [(T + C)][Mh], valid after its last force
+// evaluation: rhok itself, or (paired forward transform) unpacked into the force spectra buffer,
+// which holds nothing between steps.
+const float2* tild_half_spectra(tild_ctx* c, int s) {
+  const SysHost& h = c->sys[s];
+  const SysDev& d = c->h_sys[s];
+  if (!d.fwd_packed) return reinterpret_cast<const float2*>(c->rhok) + h.spec0;
+  float2* half = reinterpret_cast<float2*>(c->gk) + h.spec0;
+  k_unpack_half<<<nblk(h.g.Mh, 256), 256, 0, c->stream>>>(reinterpret_cast<const float2*>(c->rhok) + d.rkp0, half,
+                                                           (h.T + h.C) / 2, h.g, h.D);
+  c->launches++;
+  return half;
 }
