@@ -61,18 +61,26 @@ def test_fieldphase_forces(phase, dir_):
 
 @pytest.mark.parametrize("name", ["diblock3d_p1", "diblock3d_p3", "diblock3d_p2_odd", "diblock2d_p3", "gaussian_erf_p3"])
 def test_paired_inverse_matches_per_channel_inverse(name):
-    """Two type channels take one complex inverse transform (real part one channel's field,
-    imaginary part the other's); a fieldphase style keeps a system on the per-channel C2R inverse.
+    """Two type channels take one complex transform each way (real part one channel's field,
+    imaginary part the other's); a fieldphase style keeps a system on per-channel R2C and C2R.
     With the fieldphase at amplitude 0 the physics is the same, so both paths must agree to FP32
     rounding (odd grid edges and 2D included)."""
     s = CASES[name]()
     with tild.Context(s) as c:
         f_paired = c.forces()
+        rho_paired = c.density()
+        e_paired = c.observables()["upe"]
     s.styles = s.styles + [Style(tild.STYLE_FIELDPHASE, 0, 1, 0.0, phase=0, dir=0, n_periods=1)]
     with tild.Context(s) as c:
         f_c2r = c.forces()
+        rho_c2r = c.density()
+        e_c2r = c.observables()["upe"]
     err = rel_l2(f_paired, f_c2r)
     assert err < 1e-6, f"{name}: paired against per-channel inverse, rel L2 {err:.3e}"
+    # the forward transforms are paired too: densities (read back de-interleaved) are the same
+    # conversions bit for bit, and the energies read the unpacked spectra
+    assert np.array_equal(rho_paired, rho_c2r), name
+    assert e_paired == pytest.approx(e_c2r, rel=1e-6), name
 
 
 def test_ramp_scales_forces_like_reference():
