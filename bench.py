@@ -361,6 +361,11 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            # a timed region shorter than nvidia-smi's start-up has no sample yet: wait for the
+            # first one (at most 2 s), taken just after the region with the GPU still at its clocks
+            t0 = time.time()
+            while time.time() - t0 < 2.0 and self.out.tell() == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
