@@ -1222,10 +1222,29 @@ void launch_gather_k(tild_ctx* c, float* f_out, int f_sys, BeadRange r) {
           return;
         }
       }
+      if constexpr (!(D == 3 && P == 3)) {  // no shared memory: all of it as L1
+        static std::atomic<unsigned long long> attr_devices2{0};
+        const unsigned long long bit = 1ull << (c->device & 63);
+        if (!(attr_devices2.load() & bit)) {
+          cudaFuncSetAttribute(k_gather<D, P, I, X, CH, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxL1);
+          attr_devices2.fetch_or(bit);
+        }
+      }
       k_gather<D, P, I, X, CH, 2><<<r.n, kTile, 0, r.st>>>(  // spread ahead by global atomics
           c->pos[c->cur], c->pos[c->cur ^ 1], c->noise, c->bead_id, c->bond_nbr, c->bond_info, c->charge, c->g4,
           c->cta_bead, c->d_sys, f_out, f_sys, c->xorwow, c->field_layout, c->rho_fx, 0, c->d_status, r.off);
       return;
+    }
+  }
+  if constexpr (!(D == 3 && P == 3)) {
+    // no shared memory: all of it as L1 for the force field
+    static std::atomic<unsigned long long> attr_devices{0};  // one bit per device with the attribute set
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_devices.load() & bit)) {
+      cudaFuncSetAttribute(k_gather<D, P, I, X, CH, 0>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxL1);
+      attr_devices.fetch_or(bit);
     }
   }
   if constexpr (D == 3 && P == 3) {
