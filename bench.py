@@ -327,7 +327,7 @@ def step_bytes(s) -> int:
 # inside the timed region), doubled: the full blend has twice the beads and twice the grid
 # points, and both kernels' traffic grows in proportion.
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 2 * (119605504 + 16393216), "spread": 2 * (37655296 + 768)},
+    "blend_2.6M_128^3_gaussian_erf_p3_GJF": {"gather": 2 * (119597824 + 15529216), "spread": 2 * (37655040 + 9216)},
 }
 
 
